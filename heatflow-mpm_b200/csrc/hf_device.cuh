@@ -1,0 +1,139 @@
+// hf_device.cuh -- device-side helpers shared by the kernels of libheatflow_b200.so.
+//
+// Arithmetic contract: every binary32 expression below is evaluated in the order the reference's Warp kernels state
+// it, with one rounding per operation.  The library is compiled with -fmad=false so that nvcc does not contract a
+// multiply and an add into an FMA; divisions are IEEE round-to-nearest (-prec-div=true, the default).  That makes the
+// stencil, sampling and pointwise stages bit-identical to a serial binary32 evaluation of the same formulas.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/heatflow_b200.h"
+
+namespace hf {
+
+constexpr int kChunk = 1024;      // cells per work item
+constexpr int kThreads = 256;     // threads per block of every chunked kernel
+constexpr int kCellsPerThread = kChunk / kThreads;
+constexpr double kFxScale = 1099511627776.0;   // 2^40: particle fixed-point scale
+constexpr double kFxInv = 1.0 / 1099511627776.0;
+constexpr int kMaxScenes = 1024;
+
+struct WorkItem {
+    int scene;
+    int first;   // first cell (linear index) of the chunk
+};
+
+// ------------------------------------------------------------------------------------------ lattice arithmetic
+__device__ __forceinline__ int clampi(int i, int lo, int hi) { return i < lo ? lo : (i > hi ? hi : i); }
+__device__ __forceinline__ float minf_(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float maxf_(float a, float b) { return a > b ? a : b; }
+// Warp's clamp(x, lo, hi) = min(max(lo, x), hi)
+__device__ __forceinline__ float clampf_(float x, float lo, float hi) { return minf_(maxf_(lo, x), hi); }
+
+// fields.py:5-36 -- trilinear sample of an (nx,ny,nz) lattice with nodes at (i + off) h, indices clamped.
+__device__ __forceinline__ float sample(const float* __restrict__ a, float px, float py, float pz, float ox, float oy,
+                                        float oz, float h, int nx, int ny, int nz) {
+    float gx = __fsub_rn(__fdiv_rn(px, h), ox);
+    float gy = __fsub_rn(__fdiv_rn(py, h), oy);
+    float gz = __fsub_rn(__fdiv_rn(pz, h), oz);
+    int ix = (int)floorf(gx), iy = (int)floorf(gy), iz = (int)floorf(gz);
+    float fx = __fsub_rn(gx, (float)ix), fy = __fsub_rn(gy, (float)iy), fz = __fsub_rn(gz, (float)iz);
+    float wx0 = __fsub_rn(1.0f, fx), wy0 = __fsub_rn(1.0f, fy), wz0 = __fsub_rn(1.0f, fz);
+    int x0 = clampi(ix, 0, nx - 1), x1 = clampi(ix + 1, 0, nx - 1);
+    int y0 = clampi(iy, 0, ny - 1), y1 = clampi(iy + 1, 0, ny - 1);
+    int z0 = clampi(iz, 0, nz - 1), z1 = clampi(iz + 1, 0, nz - 1);
+    const int sy = nz, sx = ny * nz;
+    float s = 0.0f;
+    // accumulation order dx, dy, dz with weight ((wx * wy) * wz) * a, as fields.py:29-35
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(wx0, wy0), wz0), __ldg(a + x0 * sx + y0 * sy + z0)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(wx0, wy0), fz), __ldg(a + x0 * sx + y0 * sy + z1)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(wx0, fy), wz0), __ldg(a + x0 * sx + y1 * sy + z0)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(wx0, fy), fz), __ldg(a + x0 * sx + y1 * sy + z1)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(fx, wy0), wz0), __ldg(a + x1 * sx + y0 * sy + z0)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(fx, wy0), fz), __ldg(a + x1 * sx + y0 * sy + z1)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(fx, fy), wz0), __ldg(a + x1 * sx + y1 * sy + z0)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(fx, fy), fz), __ldg(a + x1 * sx + y1 * sy + z1)));
+    return s;
+}
+
+// fields.py:68-72
+__device__ __forceinline__ void sample_velocity(const float* __restrict__ u, const float* __restrict__ v,
+                                                const float* __restrict__ w, float px, float py, float pz, float h, int n,
+                                                float* o) {
+    o[0] = sample(u, px, py, pz, 0.0f, 0.5f, 0.5f, h, n + 1, n, n);
+    o[1] = sample(v, px, py, pz, 0.5f, 0.0f, 0.5f, h, n, n + 1, n);
+    o[2] = sample(w, px, py, pz, 0.5f, 0.5f, 0.0f, h, n, n, n + 1);
+}
+
+// fields.py:111-116: departure point x - dt u(x - dt/2 u(x))
+__device__ __forceinline__ void backtrace(const float* __restrict__ u, const float* __restrict__ v,
+                                          const float* __restrict__ w, const float* x, float h, int n, float dt, float* o) {
+    float vel[3];
+    sample_velocity(u, v, w, x[0], x[1], x[2], h, n, vel);
+    const float hdt = __fmul_rn(0.5f, dt);
+    float y0 = __fsub_rn(x[0], __fmul_rn(hdt, vel[0]));
+    float y1 = __fsub_rn(x[1], __fmul_rn(hdt, vel[1]));
+    float y2 = __fsub_rn(x[2], __fmul_rn(hdt, vel[2]));
+    sample_velocity(u, v, w, y0, y1, y2, h, n, vel);
+    o[0] = __fsub_rn(x[0], __fmul_rn(dt, vel[0]));
+    o[1] = __fsub_rn(x[1], __fmul_rn(dt, vel[1]));
+    o[2] = __fsub_rn(x[2], __fmul_rn(dt, vel[2]));
+}
+
+// heat.py:50-52 -- harmonic face diffusivity; symmetric bit for bit in (a, b) because 2*a is exact
+__device__ __forceinline__ float face_kappa(float a, float b) {
+    return __fdiv_rn(__fmul_rn(__fmul_rn(2.0f, a), b), __fadd_rn(__fadd_rn(a, b), 1.0e-12f));
+}
+
+// linear cell index -> (i, j, k)
+__device__ __forceinline__ void cell_ijk(int t, int n, int& i, int& j, int& k) {
+    k = t % n;
+    int q = t / n;
+    j = q % n;
+    i = q / n;
+}
+
+__device__ __forceinline__ float fx_to_float(long long v) { return __double2float_rn(__ll2double_rn(v) * kFxInv); }
+
+// ------------------------------------------------------------------------------------ deterministic block reduce
+// Sum of `v` over the block in a fixed tree (warp xor-butterfly, then warps in index order).  Result valid in every
+// thread.  `red` must hold kThreads/32 doubles per component.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* red) {
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) red[c * (kThreads / 32) + warp] = v[c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < kThreads / 32; ++q) s += red[c * (kThreads / 32) + q];
+        v[c] = s;
+    }
+}
+
+// ------------------------------------------------------------------------------------------- memory ordering
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long global_timer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+}  // namespace hf

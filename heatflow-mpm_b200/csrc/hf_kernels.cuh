@@ -1,0 +1,49 @@
+// hf_kernels.cuh -- workspace layout and kernel declarations shared by the kernel files and the host API.
+#pragma once
+
+#include "hf_device.cuh"
+
+namespace hf {
+
+// Per-scene control block of a CG solve (and the pressure-rhs mean), written by the block that finalises a scene's
+// reduction and read by every block after the following grid barrier.
+struct CgCtl {
+    double bb, rr, rz, pAp, atol_sq, mean;
+    float alpha, beta;
+    int iters, live, status, maxit;
+};
+
+// Device pointers into the caller's workspace buffer (see hf_api.cu: workspace_layout).
+struct Workspace {
+    unsigned* bar;          // [2] grid-barrier counters (reset before every persistent launch)
+    unsigned* live_count;   // [2] scenes still iterating
+    int* err;               // [1] barrier timeout flag
+    int* chunk_begin;       // [S+1] first chunk of every scene in the work table
+    CgCtl* ctl;             // [S]
+    unsigned* scene_count;  // [S] chunk arrivals in the current phase (left at 0)
+    double* partials;       // [3*C] per-chunk fp64 partial sums
+    unsigned* diag_bits;    // [4] max-reductions of the diagnostics
+};
+
+__global__ void k_scatter(const hf_scene* __restrict__ scenes, int s);
+__global__ void k_obstacle(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, int all_scenes);
+__global__ void k_coeff(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, int all_scenes);
+__global__ void k_prestage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt);
+__global__ void k_advect_T(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt);
+__global__ void k_particle_update(const hf_scene* __restrict__ scenes, int s);
+__global__ void k_face_stage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt);
+__global__ void k_divergence(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt, Workspace ws);
+__global__ void k_cell_velocity(const hf_scene* __restrict__ scenes, int s, float* __restrict__ out);
+__global__ void k_divergence_max(const hf_scene* __restrict__ scenes, int s, unsigned* __restrict__ out_bits);
+__global__ void k_speed_max(const hf_scene* __restrict__ scenes, int s, unsigned* __restrict__ out_bits);
+__global__ void k_laplacian_plain(int n, float h, float alpha, float beta, const float* __restrict__ p,
+                                  const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ az,
+                                  const float* __restrict__ y, float* __restrict__ out);
+__global__ void k_heat_matvec_plain(int n, float h, float dt, float alpha, float beta, const float* __restrict__ x,
+                                    const float* __restrict__ kap, const uint8_t* __restrict__ fl,
+                                    const float* __restrict__ y, float* __restrict__ out);
+// persistent cooperative Jacobi-PCG kernel (heat = heat system, else pressure system + projection + end of substep);
+// arguments: (const hf_scene*, const WorkItem*, int num_chunks, int num_scenes, double dt, Workspace)
+const void* pcg_kernel(bool heat);
+
+}  // namespace hf

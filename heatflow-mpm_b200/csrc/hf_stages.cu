@@ -1,0 +1,489 @@
+// hf_stages.cu -- the non-iterative stages of the air substep, batched over a scene table.
+//
+// Every chunked kernel runs one 256-thread block per 1024-cell work item (scene, first cell); each thread takes the
+// cells first + tid + 256*m, m = 0..3, so that warps read consecutive k (the contiguous axis) and every global access
+// is coalesced.  Face stages are organised by cell: a thread owns the three low faces u(i,j,k), v(i,j,k), w(i,j,k)
+// of its cell and, on the last layer, the high wall face.
+#include "hf_device.cuh"
+#include "hf_kernels.cuh"
+
+namespace hf {
+
+// ---------------------------------------------------------------------------------------------- index helpers
+__device__ __forceinline__ int uidx(int n, int i, int j, int k) { return (i * n + j) * n + k; }            // (n+1,n,n)
+__device__ __forceinline__ int vidx(int n, int i, int j, int k) { return (i * (n + 1) + j) * n + k; }      // (n,n+1,n)
+__device__ __forceinline__ int widx(int n, int i, int j, int k) { return (i * n + j) * (n + 1) + k; }      // (n,n,n+1)
+
+// ------------------------------------------------------------------------------------------------ particles
+// solver.py:19-38 (k_scatter_particles) and heat.py:12-18 (k_scatter_heat): each weight is formed in binary32
+// exactly as the reference's atomic operand, rounded to a 2^-40 fixed-point integer and added with an integer atomic,
+// so the sum does not depend on the order in which particles arrive.
+__device__ __forceinline__ void scatter_fx(long long* acc, float px, float py, float pz, float ox, float oy, float oz,
+                                           float h, int nx, int ny, int nz, float val) {
+    float gx = __fsub_rn(__fdiv_rn(px, h), ox);
+    float gy = __fsub_rn(__fdiv_rn(py, h), oy);
+    float gz = __fsub_rn(__fdiv_rn(pz, h), oz);
+    int ix = (int)floorf(gx), iy = (int)floorf(gy), iz = (int)floorf(gz);
+    float fx = __fsub_rn(gx, (float)ix), fy = __fsub_rn(gy, (float)iy), fz = __fsub_rn(gz, (float)iz);
+#pragma unroll
+    for (int dx = 0; dx < 2; ++dx) {
+        int cx = clampi(ix + dx, 0, nx - 1);
+        float wx = dx ? fx : __fsub_rn(1.0f, fx);
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy) {
+            int cy = clampi(iy + dy, 0, ny - 1);
+            float wy = dy ? fy : __fsub_rn(1.0f, fy);
+#pragma unroll
+            for (int dz = 0; dz < 2; ++dz) {
+                int cz = clampi(iz + dz, 0, nz - 1);
+                float wz = dz ? fz : __fsub_rn(1.0f, fz);
+                float c = __fmul_rn(__fmul_rn(__fmul_rn(wx, wy), wz), val);
+                long long q = __double2ll_rn((double)c * kFxScale);
+                if (q) atomicAdd(reinterpret_cast<unsigned long long*>(acc + (cx * ny + cy) * nz + cz),
+                                 static_cast<unsigned long long>(q));
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_scatter(const hf_scene* __restrict__ scenes, int s) {
+    const hf_scene& S = scenes[s];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= S.n_particles) return;
+    const int n = S.n;
+    const float h = (float)S.h, vol = (float)S.vol, k0 = (float)S.k_particle;
+    const long long M = (long long)(n + 1) * (n + 1) * (n + 1);
+    long long* acc = S.acc;
+    const float px = S.pos[3 * t], py = S.pos[3 * t + 1], pz = S.pos[3 * t + 2];
+    const float vx = S.pvel[3 * t], vy = S.pvel[3 * t + 1], vz = S.pvel[3 * t + 2];
+    const float frac = __fdiv_rn(vol, __fmul_rn(__fmul_rn(h, h), h));
+    scatter_fx(acc + 0 * M, px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n, frac);
+    scatter_fx(acc + 1 * M, px, py, pz, 0.0f, 0.5f, 0.5f, h, n + 1, n, n, __fmul_rn(frac, vx));
+    scatter_fx(acc + 2 * M, px, py, pz, 0.5f, 0.0f, 0.5f, h, n, n + 1, n, __fmul_rn(frac, vy));
+    scatter_fx(acc + 3 * M, px, py, pz, 0.5f, 0.5f, 0.0f, h, n, n, n + 1, __fmul_rn(frac, vz));
+    scatter_fx(acc + 4 * M, px, py, pz, 0.0f, 0.5f, 0.5f, h, n + 1, n, n, k0);
+    scatter_fx(acc + 5 * M, px, py, pz, 0.5f, 0.0f, 0.5f, h, n, n + 1, n, k0);
+    scatter_fx(acc + 6 * M, px, py, pz, 0.5f, 0.5f, 0.0f, h, n, n, n + 1, k0);
+    scatter_fx(acc + 7 * M, px, py, pz, 0.0f, 0.5f, 0.5f, h, n + 1, n, n, __fmul_rn(k0, vx));
+    scatter_fx(acc + 8 * M, px, py, pz, 0.5f, 0.0f, 0.5f, h, n, n + 1, n, __fmul_rn(k0, vy));
+    scatter_fx(acc + 9 * M, px, py, pz, 0.5f, 0.5f, 0.0f, h, n, n, n + 1, __fmul_rn(k0, vz));
+    scatter_fx(acc + 10 * M, px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n, frac);
+    scatter_fx(acc + 11 * M, px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n, __fmul_rn(frac, S.ptemp[t]));
+}
+
+// Obstacle fields of one substep (grid.py:202-213 plus the particle sums): reads and clears the fixed-point
+// accumulators, adds the static heater fields, zeroes the wall fluxes (grid.py:62-67).
+__device__ __forceinline__ float take(long long* acc, int idx) {
+    long long v = acc[idx];
+    if (v) acc[idx] = 0;
+    return fx_to_float(v);
+}
+
+__device__ __forceinline__ float plus_static(float a, const float* st, int idx) {
+    return st ? __fadd_rn(a, __ldg(st + idx)) : a;
+}
+
+__global__ void __launch_bounds__(kThreads) k_obstacle(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+                                                      int all_scenes) {
+    const WorkItem wi = work[blockIdx.x];
+    const hf_scene& S = scenes[wi.scene];
+    const bool particles = (S.flags & HF_FLAG_PARTICLES) && S.acc != nullptr;
+    if (!particles && !all_scenes) return;
+    const int n = S.n, N = n * n * n;
+    const long long M = (long long)(n + 1) * (n + 1) * (n + 1);
+    long long* acc = S.acc;
+    for (int m = 0; m < kCellsPerThread; ++m) {
+        const int t = wi.first + threadIdx.x + m * kThreads;
+        if (t >= N) break;
+        int i, j, k;
+        cell_ijk(t, n, i, j, k);
+        // cell lattices: alpha_s (+ static), alpha and tsum of the heat field
+        float a_s = particles ? take(acc, t) : 0.0f;
+        S.alpha_s[t] = plus_static(a_s, S.st_alpha, t);
+        S.alpha[t] = particles ? take(acc + 10 * M, t) : 0.0f;
+        S.tsum[t] = particles ? take(acc + 11 * M, t) : 0.0f;
+        // faces: low face of this cell, plus the high wall face on the last layer
+        const int fu[2] = {uidx(n, i, j, k), uidx(n, n, j, k)};
+        const int fv[2] = {vidx(n, i, j, k), vidx(n, i, n, k)};
+        const int fw[2] = {widx(n, i, j, k), widx(n, i, j, n)};
+        const bool hi[3] = {i == n - 1, j == n - 1, k == n - 1};
+        const bool lo_wall[3] = {i == 0, j == 0, k == 0};
+        float* q[3] = {S.qx, S.qy, S.qz};
+        float* kf[3] = {S.kx, S.ky, S.kz};
+        float* mf[3] = {S.mx, S.my, S.mz};
+        const float* stk[3] = {S.st_kx, S.st_ky, S.st_kz};
+        const float* stm[3] = {S.st_mx, S.st_my, S.st_mz};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int* f = a == 0 ? fu : (a == 1 ? fv : fw);
+            for (int side = 0; side < 2; ++side) {
+                if (side == 1 && !hi[a]) break;
+                const int idx = f[side];
+                const bool wall = side == 1 || lo_wall[a];
+                float qv = particles ? take(acc + (1 + a) * M, idx) : 0.0f;
+                q[a][idx] = wall ? 0.0f : qv;
+                float kv = particles ? take(acc + (4 + a) * M, idx) : 0.0f;
+                kf[a][idx] = plus_static(kv, stk[a], idx);
+                float mv = particles ? take(acc + (7 + a) * M, idx) : 0.0f;
+                mf[a][idx] = plus_static(mv, stm[a], idx);
+            }
+        }
+    }
+}
+
+// grid.py:46-59 (k_face_fraction) and heat.py:44-47 (k_conductivity) from the obstacle fields.
+__global__ void __launch_bounds__(kThreads) k_coeff(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+                                                   int all_scenes) {
+    const WorkItem wi = work[blockIdx.x];
+    const hf_scene& S = scenes[wi.scene];
+    if (!all_scenes && !(S.flags & HF_FLAG_PARTICLES)) return;
+    const int n = S.n, N = n * n * n;
+    const float afmin = (float)S.alpha_f_min, ka = (float)S.kappa_air, km = (float)S.kappa_mat;
+    const float* as = S.alpha_s;
+    for (int m = 0; m < kCellsPerThread; ++m) {
+        const int t = wi.first + threadIdx.x + m * kThreads;
+        if (t >= N) break;
+        int i, j, k;
+        cell_ijk(t, n, i, j, k);
+        const float ac = as[t];
+        S.kap[t] = __fadd_rn(ka, __fmul_rn(__fsub_rn(km, ka), clampf_(__fdiv_rn(ac, 0.6f), 0.0f, 1.0f)));
+        S.ax[uidx(n, i, j, k)] = i == 0 ? 0.0f : clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(as[t - n * n], ac))), afmin, 1.0f);
+        S.ay[vidx(n, i, j, k)] = j == 0 ? 0.0f : clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(as[t - n], ac))), afmin, 1.0f);
+        S.az[widx(n, i, j, k)] = k == 0 ? 0.0f : clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(as[t - 1], ac))), afmin, 1.0f);
+        if (i == n - 1) S.ax[uidx(n, n, j, k)] = 0.0f;
+        if (j == n - 1) S.ay[vidx(n, i, n, k)] = 0.0f;
+        if (k == n - 1) S.az[widx(n, i, j, n)] = 0.0f;
+    }
+}
+
+// --------------------------------------------------------------------------------------------- temperature
+// solver.py:74-77: k_blend (heat.py:21-28), k_apply_fixed (heat.py:147-151), k_source (heat.py:154-158) -> Tw
+__global__ void __launch_bounds__(kThreads) k_prestage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+                                                      double dt_d) {
+    const WorkItem wi = work[blockIdx.x];
+    const hf_scene& S = scenes[wi.scene];
+    const int n = S.n, N = n * n * n;
+    const int par = S.state->parity;
+    const float* T = S.T[par];
+    const bool source = (S.flags & HF_FLAG_SOURCE) != 0, particles = (S.flags & HF_FLAG_PARTICLES) != 0;
+    const float rate = (float)S.rate, t_cap = (float)S.t_cap, dt = (float)dt_d;
+    for (int m = 0; m < kCellsPerThread; ++m) {
+        const int t = wi.first + threadIdx.x + m * kThreads;
+        if (t >= N) break;
+        float tw;
+        if (particles) {
+            const float a = S.alpha[t];
+            tw = a > 0.05f ? __fdiv_rn(S.tsum[t], a) : T[t];
+        } else {
+            tw = T[t];   // alpha = 0 everywhere without particles: k_blend keeps T
+        }
+        const uint8_t fl = S.cell_flags[t];
+        if (fl & 1) tw = S.tfix[t];
+        if (source && (fl & 2)) tw = minf_(__fadd_rn(tw, __fmul_rn(rate, dt)), maxf_(tw, t_cap));
+        S.Tw[t] = tw;
+    }
+}
+
+// solver.py:78 k_advect (heat.py:31-41) into T[parity^1], fused with k_heat_rhs (heat.py:108-118) which only needs
+// the advected value of the same cell.
+__global__ void __launch_bounds__(kThreads) k_advect_T(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+                                                      double dt_d) {
+    const WorkItem wi = work[blockIdx.x];
+    const hf_scene& S = scenes[wi.scene];
+    const int n = S.n, N = n * n * n;
+    const int par = S.state->parity;
+    const float *u = S.u[par], *v = S.v[par], *w = S.w[par];
+    float* T2 = S.T[par ^ 1];
+    const float h = (float)S.h, dt = (float)dt_d;
+    const float* Tw = S.Tw;
+    const float* kap = S.kap;
+    const uint8_t* fl = S.cell_flags;
+    const float c_dt = __fdiv_rn(dt, __fmul_rn(h, h));
+    for (int m = 0; m < kCellsPerThread; ++m) {
+        const int t = wi.first + threadIdx.x + m * kThreads;
+        if (t >= N) break;
+        int i, j, k;
+        cell_ijk(t, n, i, j, k);
+        float out;
+        if (S.alpha_s[t] > 0.5f) {
+            out = Tw[t];
+        } else {
+            float x[3] = {__fmul_rn(__fadd_rn((float)i, 0.5f), h), __fmul_rn(__fadd_rn((float)j, 0.5f), h),
+                          __fmul_rn(__fadd_rn((float)k, 0.5f), h)};
+            float y[3];
+            backtrace(u, v, w, x, h, n, dt, y);
+            out = sample(Tw, y[0], y[1], y[2], 0.5f, 0.5f, 0.5f, h, n, n, n);
+        }
+        T2[t] = out;
+        // heat rhs: tfix on fixed cells, else T2 + dt/h^2 * sum over fixed neighbours of kappa_f * tfix
+        float rhs;
+        if (fl[t] & 1) {
+            rhs = S.tfix[t];
+        } else {
+            const float kc = kap[t];
+            float acc = 0.0f;
+            const int nbr[6] = {t - n * n, t + n * n, t - n, t + n, t - 1, t + 1};
+            const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                if (!in[s]) continue;
+                const int nb = nbr[s];
+                if (fl[nb] & 1) acc = __fadd_rn(acc, __fmul_rn(face_kappa(kc, kap[nb]), S.tfix[nb]));
+            }
+            rhs = __fadd_rn(out, __fmul_rn(c_dt, acc));
+        }
+        S.hrhs[t] = rhs;
+    }
+}
+
+// heat.py:161-174 k_particle_update: FLIP increment between Tw and the diffused T, melt law
+__global__ void __launch_bounds__(kThreads) k_particle_update(const hf_scene* __restrict__ scenes, int s) {
+    const hf_scene& S = scenes[s];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= S.n_particles) return;
+    const int n = S.n, par = S.state->parity;
+    const float h = (float)S.h;
+    const float t_sol = (float)S.t_sol, t_liq = (float)S.t_liq, y_solid = (float)S.y_solid;
+    const float mu_s = (float)S.mu_s, mu_l = (float)S.mu_l, t_max = (float)S.t_max;
+    const float px = S.pos[3 * t], py = S.pos[3 * t + 1], pz = S.pos[3 * t + 2];
+    const float dT = __fsub_rn(sample(S.T[par ^ 1], px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n),
+                               sample(S.Tw, px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n));
+    const float tp = clampf_(__fadd_rn(S.ptemp[t], dT), 0.0f, t_max);
+    S.ptemp[t] = tp;
+    const float f = clampf_(__fdiv_rn(__fsub_rn(tp, t_sol), __fsub_rn(t_liq, t_sol)), 0.0f, 1.0f);
+    S.pmelt[t] = f;
+    S.pyield[t] = __fmul_rn(y_solid, __fsub_rn(1.0f, f));
+    S.pvisc[t] = __fadd_rn(__fmul_rn(mu_s, __fsub_rn(1.0f, f)), __fmul_rn(mu_l, f));
+}
+
+// ------------------------------------------------------------------------------------------------ air faces
+// grid.py:219-233 for the faces of one cell: k_advect_face from the old u,v,w (grid.py:25-33), k_buoyancy on w
+// (grid.py:36-43, with the new T), k_relax (grid.py:70-79).  Each face's value depends only on its own intermediate
+// values, so applying the three kernels face by face is the same arithmetic as the reference's three passes.
+__device__ __forceinline__ float relax_face(float q, float af, float kf, float mf, float rho, float afmin, float h,
+                                            float dt) {
+    const float c = __fdiv_rn(1.0f, __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(rho, maxf_(af, afmin)), h), h), h));
+    const float dtc = __fmul_rn(dt, c);
+    return __fdiv_rn(__fadd_rn(q, __fmul_rn(dtc, mf)), __fadd_rn(1.0f, __fmul_rn(dtc, kf)));
+}
+
+__global__ void __launch_bounds__(kThreads) k_face_stage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+                                                        double dt_d) {
+    const WorkItem wi = work[blockIdx.x];
+    const hf_scene& S = scenes[wi.scene];
+    const int n = S.n, N = n * n * n;
+    const int par = S.state->parity;
+    const float *u0 = S.u[par], *v0 = S.v[par], *w0 = S.w[par];
+    float *u1 = S.u[par ^ 1], *v1 = S.v[par ^ 1], *w1 = S.w[par ^ 1];
+    const float* Tn = S.T[par ^ 1];
+    const float h = (float)S.h, dt = (float)dt_d, rho = (float)S.rho, afmin = (float)S.alpha_f_min;
+    const float g = (float)S.g, t_amb = (float)S.t_amb;
+    const bool buoy = (S.flags & HF_FLAG_BUOYANCY) != 0;
+    const float buoy_num = __fmul_rn(dt, g), buoy_den = __fadd_rn(t_amb, 273.15f);
+    for (int m = 0; m < kCellsPerThread; ++m) {
+        const int t = wi.first + threadIdx.x + m * kThreads;
+        if (t >= N) break;
+        int i, j, k;
+        cell_ijk(t, n, i, j, k);
+        const float fi = (float)i, fj = (float)j, fk = (float)k;
+        const float ci = __fmul_rn(__fadd_rn(fi, 0.5f), h), cj = __fmul_rn(__fadd_rn(fj, 0.5f), h),
+                    ck = __fmul_rn(__fadd_rn(fk, 0.5f), h);
+        float y[3];
+        // u(i,j,k)
+        {
+            const int f = uidx(n, i, j, k);
+            float val = 0.0f;
+            if (i != 0) {
+                const float x[3] = {__fmul_rn(fi, h), cj, ck};
+                backtrace(u0, v0, w0, x, h, n, dt, y);
+                val = sample(u0, y[0], y[1], y[2], 0.0f, 0.5f, 0.5f, h, n + 1, n, n);
+                val = relax_face(val, S.ax[f], S.kx[f], S.mx[f], rho, afmin, h, dt);
+            }
+            u1[f] = val;
+            if (i == n - 1) u1[uidx(n, n, j, k)] = 0.0f;
+        }
+        // v(i,j,k)
+        {
+            const int f = vidx(n, i, j, k);
+            float val = 0.0f;
+            if (j != 0) {
+                const float x[3] = {ci, __fmul_rn(fj, h), ck};
+                backtrace(u0, v0, w0, x, h, n, dt, y);
+                val = sample(v0, y[0], y[1], y[2], 0.5f, 0.0f, 0.5f, h, n, n + 1, n);
+                val = relax_face(val, S.ay[f], S.ky[f], S.my[f], rho, afmin, h, dt);
+            }
+            v1[f] = val;
+            if (j == n - 1) v1[vidx(n, i, n, k)] = 0.0f;
+        }
+        // w(i,j,k)
+        {
+            const int f = widx(n, i, j, k);
+            float val = 0.0f;
+            if (k != 0) {
+                const float x[3] = {ci, cj, __fmul_rn(fk, h)};
+                backtrace(u0, v0, w0, x, h, n, dt, y);
+                val = sample(w0, y[0], y[1], y[2], 0.5f, 0.5f, 0.0f, h, n, n, n + 1);
+                if (buoy) {
+                    const float tf = __fmul_rn(0.5f, __fadd_rn(Tn[t - 1], Tn[t]));
+                    val = __fadd_rn(val, __fdiv_rn(__fmul_rn(buoy_num, __fsub_rn(tf, t_amb)), buoy_den));
+                }
+                val = relax_face(val, S.az[f], S.kz[f], S.mz[f], rho, afmin, h, dt);
+            }
+            w1[f] = val;
+            if (k == n - 1) w1[widx(n, i, j, n)] = 0.0f;
+        }
+    }
+}
+
+// grid.py:82-91 k_divergence_rhs with scale rho/dt into rhs, plus the fp64 partial sum of the chunk for the mean of
+// grid.py:238-241 (reduced over the scene by the pressure CG kernel, in a fixed tree).
+__global__ void __launch_bounds__(kThreads) k_divergence(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+                                                        double dt_d, Workspace ws) {
+    __shared__ double red[kThreads / 32];
+    const int c = blockIdx.x;
+    const WorkItem wi = work[c];
+    const hf_scene& S = scenes[wi.scene];
+    const int n = S.n, N = n * n * n;
+    const int par = S.state->parity;
+    const float *u = S.u[par ^ 1], *v = S.v[par ^ 1], *w = S.w[par ^ 1];
+    const float h = (float)S.h, scale = (float)(S.rho / dt_d);
+    double part[1] = {0.0};
+    for (int m = 0; m < kCellsPerThread; ++m) {
+        const int t = wi.first + threadIdx.x + m * kThreads;
+        if (t >= N) break;
+        int i, j, k;
+        cell_ijk(t, n, i, j, k);
+        const int u0 = uidx(n, i, j, k), u1i = uidx(n, i + 1, j, k);
+        const int v0 = vidx(n, i, j, k), v1i = vidx(n, i, j + 1, k);
+        const int w0 = widx(n, i, j, k), w1i = w0 + 1;
+        float d = __fmul_rn(S.ax[u1i], u[u1i]);
+        d = __fadd_rn(d, S.qx[u1i]);
+        d = __fsub_rn(d, __fmul_rn(S.ax[u0], u[u0]));
+        d = __fsub_rn(d, S.qx[u0]);
+        d = __fadd_rn(d, __fmul_rn(S.ay[v1i], v[v1i]));
+        d = __fadd_rn(d, S.qy[v1i]);
+        d = __fsub_rn(d, __fmul_rn(S.ay[v0], v[v0]));
+        d = __fsub_rn(d, S.qy[v0]);
+        d = __fadd_rn(d, __fmul_rn(S.az[w1i], w[w1i]));
+        d = __fadd_rn(d, S.qz[w1i]);
+        d = __fsub_rn(d, __fmul_rn(S.az[w0], w[w0]));
+        d = __fsub_rn(d, S.qz[w0]);
+        d = __fdiv_rn(d, h);
+        const float r = __fmul_rn(-scale, d);
+        S.rhs[t] = r;
+        part[0] += (double)r;
+    }
+    block_sum<1>(part, red);
+    if (threadIdx.x == 0) ws.partials[3 * c] = part[0];
+}
+
+// ---------------------------------------------------------------------------------------------- diagnostics
+// grid.py:156-162 k_cell_velocity
+__global__ void k_cell_velocity(const hf_scene* __restrict__ scenes, int s, float* __restrict__ out) {
+    const hf_scene& S = scenes[s];
+    const int n = S.n, N = n * n * n, par = S.state->parity;
+    const float *u = S.u[par], *v = S.v[par], *w = S.w[par];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_ijk(t, n, i, j, k);
+        out[3 * t + 0] = __fmul_rn(0.5f, __fadd_rn(u[uidx(n, i, j, k)], u[uidx(n, i + 1, j, k)]));
+        out[3 * t + 1] = __fmul_rn(0.5f, __fadd_rn(v[vidx(n, i, j, k)], v[vidx(n, i, j + 1, k)]));
+        out[3 * t + 2] = __fmul_rn(0.5f, __fadd_rn(w[widx(n, i, j, k)], w[widx(n, i, j, k) + 1]));
+    }
+}
+
+// grid.py:257-260 divergence_max (k_divergence_rhs with scale 1, max |.| * h) and grid.py:262-263 speed_max.
+// Non-negative floats order like their bit patterns, so atomicMax on the bits gives the maximum.
+__global__ void k_divergence_max(const hf_scene* __restrict__ scenes, int s, unsigned* __restrict__ out_bits) {
+    const hf_scene& S = scenes[s];
+    const int n = S.n, N = n * n * n, par = S.state->parity;
+    const float *u = S.u[par], *v = S.v[par], *w = S.w[par];
+    const float h = (float)S.h;
+    float mx = 0.0f;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_ijk(t, n, i, j, k);
+        const int u0 = uidx(n, i, j, k), u1i = uidx(n, i + 1, j, k);
+        const int v0 = vidx(n, i, j, k), v1i = vidx(n, i, j + 1, k);
+        const int w0 = widx(n, i, j, k), w1i = w0 + 1;
+        float d = __fmul_rn(S.ax[u1i], u[u1i]);
+        d = __fadd_rn(d, S.qx[u1i]);
+        d = __fsub_rn(d, __fmul_rn(S.ax[u0], u[u0]));
+        d = __fsub_rn(d, S.qx[u0]);
+        d = __fadd_rn(d, __fmul_rn(S.ay[v1i], v[v1i]));
+        d = __fadd_rn(d, S.qy[v1i]);
+        d = __fsub_rn(d, __fmul_rn(S.ay[v0], v[v0]));
+        d = __fsub_rn(d, S.qy[v0]);
+        d = __fadd_rn(d, __fmul_rn(S.az[w1i], w[w1i]));
+        d = __fadd_rn(d, S.qz[w1i]);
+        d = __fsub_rn(d, __fmul_rn(S.az[w0], w[w0]));
+        d = __fsub_rn(d, S.qz[w0]);
+        d = __fdiv_rn(d, h);
+        mx = fmaxf(mx, fabsf(__fmul_rn(-1.0f, d)));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_uint(mx));
+}
+
+__global__ void k_speed_max(const hf_scene* __restrict__ scenes, int s, unsigned* __restrict__ out_bits) {
+    const hf_scene& S = scenes[s];
+    const int n = S.n, par = S.state->parity;
+    const int NF = (n + 1) * n * n;
+    float mx = 0.0f;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < NF; t += gridDim.x * blockDim.x)
+        mx = fmaxf(mx, fmaxf(fabsf(S.u[par][t]), fmaxf(fabsf(S.v[par][t]), fabsf(S.w[par][t]))));
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_uint(mx));
+}
+
+// ------------------------------------------------------------------------------------- single-kernel parity
+// grid.py:94-115 k_laplacian on plain arrays
+__global__ void k_laplacian_plain(int n, float h, float alpha, float beta, const float* __restrict__ p,
+                                  const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ az,
+                                  const float* __restrict__ y, float* __restrict__ out) {
+    const int N = n * n * n, nn = n * n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_ijk(t, n, i, j, k);
+        const float pc = p[t];
+        float acc = 0.0f;
+        if (i > 0) acc = __fadd_rn(acc, __fmul_rn(ax[uidx(n, i, j, k)], __fsub_rn(pc, p[t - nn])));
+        if (i < n - 1) acc = __fadd_rn(acc, __fmul_rn(ax[uidx(n, i + 1, j, k)], __fsub_rn(pc, p[t + nn])));
+        if (j > 0) acc = __fadd_rn(acc, __fmul_rn(ay[vidx(n, i, j, k)], __fsub_rn(pc, p[t - n])));
+        if (j < n - 1) acc = __fadd_rn(acc, __fmul_rn(ay[vidx(n, i, j + 1, k)], __fsub_rn(pc, p[t + n])));
+        if (k > 0) acc = __fadd_rn(acc, __fmul_rn(az[widx(n, i, j, k)], __fsub_rn(pc, p[t - 1])));
+        if (k < n - 1) acc = __fadd_rn(acc, __fmul_rn(az[widx(n, i, j, k + 1)], __fsub_rn(pc, p[t + 1])));
+        out[t] = __fadd_rn(__fdiv_rn(__fmul_rn(alpha, acc), __fmul_rn(h, h)), __fmul_rn(beta, y[t]));
+    }
+}
+
+// heat.py:94-105 k_heat_matvec on plain arrays
+__global__ void k_heat_matvec_plain(int n, float h, float dt, float alpha, float beta, const float* __restrict__ x,
+                                    const float* __restrict__ kap, const uint8_t* __restrict__ fl,
+                                    const float* __restrict__ y, float* __restrict__ out) {
+    const int N = n * n * n, nn = n * n;
+    const float c_dt = __fdiv_rn(dt, __fmul_rn(h, h));
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
+        int i, j, k;
+        cell_ijk(t, n, i, j, k);
+        const float xc = x[t];
+        if (fl[t] & 1) {
+            out[t] = __fadd_rn(__fmul_rn(alpha, xc), __fmul_rn(beta, y[t]));
+            continue;
+        }
+        const float kc = kap[t];
+        float acc = 0.0f;
+        const int nbr[6] = {t - nn, t + nn, t - n, t + n, t - 1, t + 1};
+        const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            if (!in[s]) continue;
+            const int nb = nbr[s];
+            const float kf = face_kappa(kc, kap[nb]);
+            acc = __fadd_rn(acc, (fl[nb] & 1) ? __fmul_rn(kf, xc) : __fmul_rn(kf, __fsub_rn(xc, x[nb])));
+        }
+        out[t] = __fadd_rn(__fmul_rn(alpha, __fadd_rn(xc, __fmul_rn(c_dt, acc))), __fmul_rn(beta, y[t]));
+    }
+}
+
+}  // namespace hf

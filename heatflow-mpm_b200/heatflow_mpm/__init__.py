@@ -1,0 +1,8 @@
+"""heatflow_mpm on B200: the Eulerian air substep of Heatflow-MPM as sm_100a CUDA behind the reference's Python API."""
+from .grid import GridConfig, AirGrid  # noqa: F401
+from .heat import HeatField  # noqa: F401
+from .heater import Heater, BoxHeater  # noqa: F401
+from .mpm import Material, ThermalMPM, FrozenBody  # noqa: F401
+from .solver import HeatflowMPM, KAPPA_AIR  # noqa: F401
+
+__version__ = "0.2.0"

@@ -1,0 +1,168 @@
+/*
+ * heatflow_b200.h -- C ABI of libheatflow_b200.so, the sm_100a implementation of Heatflow-MPM's Eulerian air substep.
+ *
+ * Every entry point takes plain pointers, sizes and a cudaStream_t (passed as void*), returns an hf_status, never
+ * synchronises the stream on its own (the set-up calls that upload tables say so), and never allocates device memory:
+ * all device buffers -- fields, the scene table, the work table and the workspace -- belong to the caller.
+ *
+ * The reference (pietis/Heatflow-MPM) has no native layer: every stage is a Warp kernel launched from Python.  Each
+ * entry point below names the reference function or kernels it replaces (file:line within that repository).
+ *
+ * Data layout (identical to the reference's Warp arrays, C order, k fastest):
+ *   cell fields (n,n,n) float32; u (n+1,n,n), v (n,n+1,n), w (n,n,n+1) float32; particle positions/velocities (P,3).
+ *   cell flags (n,n,n) uint8: bit0 = fixed (Dirichlet) cell, bit1 = heater source cell.
+ * The temperature T and the face velocities u,v,w are double-buffered: buffer [parity] is current, where parity is
+ * the scene's device-side hf_scene_state.parity, flipped by the last stage of every substep (so a captured CUDA graph
+ * of a substep can be replayed without re-recording).
+ */
+#ifndef HEATFLOW_B200_H
+#define HEATFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HF_ABI_VERSION 1
+
+typedef enum hf_status {
+    HF_OK = 0,
+    HF_ERR_ARG = 1,        /* invalid argument (null pointer, size out of range, misaligned buffer) */
+    HF_ERR_CUDA = 2,       /* a CUDA runtime call failed; hf_last_error() has the text */
+    HF_ERR_WORKSPACE = 3,  /* workspace smaller than hf_workspace_bytes() */
+    HF_ERR_DEVICE = 4      /* no sm_100 device, or a cooperative launch cannot fit the grid */
+} hf_status;
+
+/* per-scene solver status word, in hf_scene_state.status (bit set) */
+#define HF_SCENE_OK 0
+#define HF_SCENE_HEAT_MAXITER 1      /* heat CG stopped at maxiter above its tolerance */
+#define HF_SCENE_PRESSURE_MAXITER 2  /* pressure CG stopped at maxiter above its tolerance */
+#define HF_SCENE_NONFINITE 4         /* a CG residual became NaN/inf */
+#define HF_SCENE_BARRIER_TIMEOUT 8   /* a grid barrier of a persistent kernel gave up (bounded wait) */
+
+/* hf_scene.flags */
+#define HF_FLAG_BUOYANCY 1u          /* GridConfig.buoyancy (grid.py:18) */
+#define HF_FLAG_SOURCE 2u            /* heater source active: rate > 0 (solver.py:76) */
+#define HF_FLAG_PARTICLES 4u         /* particle coupling on: obstacle fields rebuilt every substep (solver.py:65-72) */
+#define HF_FLAG_ACTIVE 8u            /* scene takes part in batched calls (serving slots) */
+
+/* Mutable device-side state of one scene (caller allocates sizeof(hf_scene_state) bytes of device memory, zeroed). */
+typedef struct hf_scene_state {
+    int32_t parity;        /* index of the current T / u,v,w buffer */
+    int32_t status;        /* HF_SCENE_* bits of the last substep */
+    int64_t substeps;      /* substeps completed */
+    int32_t heat_iters;    /* heat CG iterations performed in the last substep (HeatField.cg_iters, heat.py:210) */
+    int32_t pressure_iters;/* pressure CG iterations performed in the last substep (AirGrid.cg_iters, grid.py:249) */
+    double heat_rr, heat_atol;       /* final r.r and absolute tolerance of the heat solve */
+    double pressure_rr, pressure_atol;
+    double pressure_bb, heat_bb;     /* b.b of the last solves (||r||/||b|| = sqrt(rr/bb)) */
+    double rhs_mean;                 /* mean removed from the pressure rhs (grid.py:238-241) */
+    int64_t total_heat_iters, total_pressure_iters;
+    double reserved[4];
+} hf_scene_state;
+
+/* One scene: sizes, physical parameters and device pointers of its fields.  The same struct is the element of the
+ * device-side scene table (hf_plan.scenes_dev); it holds no host pointers. */
+typedef struct hf_scene {
+    int32_t n;                 /* cells per edge (AirGrid.n, grid.py:183) */
+    int32_t n_particles;       /* material particles (0: air-only) */
+    uint32_t flags;            /* HF_FLAG_* */
+    int32_t cg_max_iter;       /* GridConfig.cg_max_iter (400) */
+    int32_t heat_maxiter;      /* HeatField.diffuse maxiter (200) */
+    int32_t reserved_i[3];
+    /* Physical parameters as the reference's Python floats (double).  Kernels round them to binary32 exactly where
+     * Warp does at launch; derived scalars (rho/dt, dt/rho) are formed in double first, as the Python code does. */
+    double h, rho, t_amb, alpha_f_min, g;          /* GridConfig (grid.py:13-22); g = 9.81 (grid.py:219) */
+    double cg_tol, heat_tol;                       /* relative CG tolerances (grid.py:21; heat.py:198) */
+    double kappa_air, kappa_mat;                   /* thermal diffusivities (solver.py:15; mpm.py:17) */
+    double rate, t_cap;                            /* heater source rate [K/s] and cap (heater.py:51-52) */
+    double vol, k_particle;                        /* particle volume spacing^3 and K_PARTICLE (solver.py:16) */
+    double t_sol, t_liq, y_solid, mu_s, mu_l, t_max; /* melt law (heat.py:161-174) */
+    /* double-buffered state */
+    float *T[2];
+    float *u[2], *v[2], *w[2];
+    /* temperature stage */
+    float *Tw, *kap, *hrhs, *hdiag, *tfix, *alpha, *tsum;
+    uint8_t *cell_flags;
+    /* air grid */
+    float *p, *rhs, *pdiag, *alpha_s;
+    float *ax, *ay, *az, *qx, *qy, *qz, *kx, *ky, *kz, *mx, *my, *mz;
+    /* static obstacle fields (heater body), added every substep (grid.py:206-213); NULL = none */
+    float *st_alpha, *st_kx, *st_ky, *st_kz, *st_mx, *st_my, *st_mz;
+    /* CG vectors (n^3 each): residual, preconditioned residual, search direction (2 buffers), A*p */
+    float *cg_r, *cg_z, *cg_p[2], *cg_Ap;
+    /* particles (P,3) / (P): positions and velocities in, temperature/melt/yield/viscosity in-out */
+    float *pos, *pvel, *ptemp, *pmelt, *pyield, *pvisc;
+    /* 12 fixed-point accumulators of (n+1)^3 int64 each (coupled scenes only), zero on entry, left zero */
+    long long *acc;
+    hf_scene_state *state;
+} hf_scene;
+
+/* A batch of scenes ready to launch: tables in device memory plus the host copy used to size launches. */
+typedef struct hf_plan {
+    int32_t num_scenes;
+    int32_t num_chunks;        /* 1024-cell work items over all scenes */
+    const hf_scene *scenes_host;   /* host copy, valid while the plan is used */
+    void *scenes_dev;          /* device: hf_scene[num_scenes] */
+    void *work_dev;            /* device: int32 pairs (scene, first cell) [num_chunks] */
+    void *workspace;           /* device: >= hf_workspace_bytes(num_scenes, num_chunks) bytes */
+    size_t workspace_bytes;
+    int32_t persistent_blocks; /* grid of the persistent CG kernels (0 = choose: SMs x occupancy) */
+    int32_t reserved;
+} hf_plan;
+
+/* ---------------------------------------------------------------------------------------------------- set-up */
+int hf_abi_version(void);
+const char *hf_last_error(void);
+int hf_cells_per_chunk(void);
+/* workspace bytes for a plan of num_scenes scenes and num_chunks chunks */
+size_t hf_workspace_bytes(int num_scenes, int num_chunks);
+/* number of 1024-cell chunks of a scene of n cells per edge */
+int hf_chunks_for(int n);
+/* Writes the scene table and the work table to the device and fills plan.num_chunks.  Blocking: the stream is
+ * synchronised before return (set-up call, not for the per-substep path). */
+int hf_plan_upload(hf_plan *plan, void *stream);
+
+/* --------------------------------------------------------------------------------- per-substep stages (batched) */
+/* solver.py:65-72 + grid.py:202-213 + grid.py:46-67 + heat.py:44-47: obstacle fields of every scene -- particle
+ * scatter (k_scatter_particles solver.py:19-38, k_scatter_heat heat.py:12-18) into fixed-point accumulators, plus the
+ * static heater fields, face fractions alpha_f with zeroed wall fluxes, and the conductivity kappa.  Scenes without
+ * HF_FLAG_PARTICLES are skipped unless `all_scenes` is set (used once at set-up to fill their static fields). */
+int hf_obstacle_fields(const hf_plan *plan, int all_scenes, void *stream);
+/* solver.py:74-79 + heat.py:108-118: k_blend, k_apply_fixed, k_source (rate > 0), k_advect, k_heat_rhs */
+int hf_temperature_stage(const hf_plan *plan, double dt, void *stream);
+/* heat.py:198-210: k_heat_diag + warp.optim.linear.cg(k_heat_matvec, M = diag, tol, maxiter, check_every=10),
+ * solved in place in T[parity^1] by one persistent cooperative kernel with device-side convergence */
+int hf_heat_solve(const hf_plan *plan, double dt, void *stream);
+/* heat.py:161-174 k_particle_update (FLIP increment, melt fraction, yield stress, viscosity) */
+int hf_particle_update(const hf_plan *plan, void *stream);
+/* grid.py:219-233: k_advect_face x3 (into u,v,w[parity^1]), k_buoyancy, k_relax x3 */
+int hf_face_stage(const hf_plan *plan, double dt, void *stream);
+/* grid.py:235-251 + 140-153: k_divergence_rhs, device-side mean removal (replaces the host read-back of
+ * grid.py:239), k_jacobi, warp.optim.linear.cg(k_laplacian, check_every=20) warm-started from p, k_project x3; then
+ * flips every scene's parity (end of substep) */
+int hf_pressure_solve(const hf_plan *plan, double dt, void *stream);
+/* the whole air substep in order (solver.py:63-88 minus the MPM step) */
+int hf_substep(const hf_plan *plan, double dt, void *stream);
+
+/* ------------------------------------------------------------------------------------------ getters (one scene) */
+/* grid.py:156-162 k_cell_velocity: out (n^3,3) float32 from u,v,w[parity] of scene `s` (host copy of the table) */
+int hf_cell_velocity(const hf_plan *plan, int s, float *out, void *stream);
+/* grid.py:257-263: max|div(alpha_f u + q)| * h and max |u|,|v|,|w|; result written to out_dev[0] (float, device) */
+int hf_divergence_max(const hf_plan *plan, int s, float *out_dev, void *stream);
+int hf_speed_max(const hf_plan *plan, int s, float *out_dev, void *stream);
+
+/* ------------------------------------------------------------- single-kernel entry points (parity, unit tests) */
+/* grid.py:94-115 k_laplacian: out = alpha * L(p) / h^2 + beta * y (n^3 arrays, one scene) */
+int hf_k_laplacian(int n, double h, double alpha, double beta, const float *p, const float *ax, const float *ay,
+                   const float *az, const float *y, float *out, void *stream);
+/* heat.py:94-105 k_heat_matvec */
+int hf_k_heat_matvec(int n, double h, double dt, double alpha, double beta, const float *x, const float *kap,
+                     const uint8_t *cell_flags, const float *y, float *out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HEATFLOW_B200_H */

@@ -1,0 +1,64 @@
+"""The reference's physics tests (tests/test_solver.py:21-46 of pietis/Heatflow-MPM), unchanged in setup and
+thresholds, run through this package on the GPU.  They are the reference's only known-answer tests of the air path:
+the erfc conduction profile pins the heat CG, the rising plume pins buoyancy/advection/projection and the heater
+source, the fan test pins the fan relaxation and the advection of T."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NONE = np.zeros((0, 3), np.float32)
+DEV = "cuda:0"
+
+
+def run(sim, seconds, dt=2e-3):
+    for _ in range(int(seconds / dt)):
+        sim.substep(dt)
+
+
+def test_implicit_conduction_matches_erfc():
+    from heatflow_mpm import HeatflowMPM, Heater, GridConfig
+    sim = HeatflowMPM(NONE, heater=Heater(on=False), grid=GridConfig(L=0.30, buoyancy=False), kappa_air=1e-3, device=DEV)
+    n = sim.grid.n
+    fixed = np.zeros((n, n, n), bool)
+    fixed[:, :, 0] = True
+    sim.heat.set_fixed(fixed, np.where(fixed, 70.0, 0.0))
+    run(sim, 2.0)
+    T = sim.grid_T()[n // 2, n // 2, :]
+    z = np.maximum((np.arange(n) + 0.5) * sim.grid.h - sim.grid.h / 2, 0.0)
+    ref = 25.0 + 45.0 * np.array([math.erfc(v / (2 * math.sqrt(1e-3 * 2.0))) for v in z])
+    assert np.abs(T - ref)[: n // 2].max() < 0.1
+
+
+def test_heater_plume_rises():
+    from heatflow_mpm import HeatflowMPM, Heater
+    sim = HeatflowMPM(NONE, heater=Heater(power=400.0, t_cap=120.0), device=DEV)
+    run(sim, 3.0)
+    T = sim.grid_T()
+    hc = sim.heater_geom["centre"]
+    i, j = int(hc[0] / sim.grid.h), int(hc[1] / sim.grid.h)
+    assert np.isfinite(T).all() and sim.grid.speed_max() > 0.2
+    assert T[i, j, sim.grid.n - 2] > sim.grid.cfg.t_amb + 3.0
+    assert sim.grid.divergence_max() < 1e-3
+
+
+def test_fan_heats_the_material_position():
+    from heatflow_mpm import HeatflowMPM, Heater
+    sim = HeatflowMPM(NONE, heater=Heater(power=400.0, t_cap=120.0, fan=2.0), device=DEV)
+    run(sim, 3.0)
+    T = sim.grid_T()
+    c = sim.grid.n // 2
+    kb = int(0.05 / sim.grid.h)
+    assert max(T[c, c, kb], T[c, c, kb + 4]) > 40.0
+
+
+def test_cold_solid_holds_its_shape():
+    """tests/test_solver.py:49-54 needs Newton (skipped without it, as in the reference)."""
+    pytest.importorskip("newton")
+    from heatflow_mpm import HeatflowMPM, Heater
+    from heatflow_mpm.shapes import mesh_particles
+    sim = HeatflowMPM(mesh_particles(device=DEV), heater=Heater(on=False), t_init=20.0, device=DEV)
+    run(sim, 1.0)
+    assert sim.temperatures().max() < sim.mat.t_sol and sim.melt_fraction().max() == 0.0
