@@ -268,7 +268,7 @@ int hf_face_stage(const hf_plan* p, double dt, void* stream) {
     return HF_OK;
 }
 
-int hf_pressure_solve(const hf_plan* p, double dt, void* stream) {
+int hf_divergence_stage(const hf_plan* p, double dt, void* stream) {
     int rc = check_plan(p);
     if (rc) return rc;
     if (!p->num_chunks) return HF_OK;
@@ -276,7 +276,19 @@ int hf_pressure_solve(const hf_plan* p, double dt, void* stream) {
                                                                    static_cast<const hf::WorkItem*>(p->work_dev), dt,
                                                                    workspace(p));
     HF_CUDA(cudaGetLastError(), "launch (divergence)");
+    return HF_OK;
+}
+
+int hf_pressure_cg(const hf_plan* p, double dt, void* stream) {
+    int rc = check_plan(p);
+    if (rc) return rc;
     return launch_pcg(p, false, dt, stream);
+}
+
+int hf_pressure_solve(const hf_plan* p, double dt, void* stream) {
+    int rc = hf_divergence_stage(p, dt, stream);
+    if (rc) return rc;
+    return hf_pressure_cg(p, dt, stream);
 }
 
 int hf_substep(const hf_plan* p, double dt, void* stream) {

@@ -72,7 +72,8 @@ def load():
     L.hf_workspace_bytes.argtypes = [C.c_int, C.c_int]
     L.hf_chunks_for.argtypes = [C.c_int]
     L.hf_plan_upload.argtypes = [C.POINTER(Plan), _P]
-    for name in ("hf_temperature_stage", "hf_heat_solve", "hf_face_stage", "hf_pressure_solve", "hf_substep"):
+    for name in ("hf_temperature_stage", "hf_heat_solve", "hf_face_stage", "hf_pressure_solve", "hf_substep",
+                 "hf_divergence_stage", "hf_pressure_cg"):
         getattr(L, name).argtypes = [C.POINTER(Plan), C.c_double, _P]
     L.hf_obstacle_fields.argtypes = [C.POINTER(Plan), C.c_int, _P]
     L.hf_particle_update.argtypes = [C.POINTER(Plan), _P]

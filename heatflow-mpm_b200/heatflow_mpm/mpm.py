@@ -41,6 +41,11 @@ class FrozenBody:
     def particle_state(self):
         return self.pos_t, self.vel_t
 
+    def set_state(self, positions, velocities):
+        """Replace the particle state (host arrays or tensors; pinned host tensors copy asynchronously)."""
+        self.pos_t.copy_(torch.as_tensor(positions), non_blocking=True)
+        self.vel_t.copy_(torch.as_tensor(velocities), non_blocking=True)
+
     def material_outputs(self):
         return self.yield_t, self.visc_t
 

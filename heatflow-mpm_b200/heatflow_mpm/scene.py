@@ -270,6 +270,12 @@ class ScenePlan:
     def pressure_solve(self, dt):
         self._call("hf_pressure_solve", float(dt))
 
+    def divergence_stage(self, dt):
+        self._call("hf_divergence_stage", float(dt))
+
+    def pressure_cg(self, dt):
+        self._call("hf_pressure_cg", float(dt))
+
     def cell_velocity(self, s=0):
         sc = self.scenes[s]
         out = torch.empty((sc.n ** 3, 3), dtype=F32, device=self.device)

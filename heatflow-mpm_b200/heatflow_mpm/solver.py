@@ -33,6 +33,24 @@ def wall_fixed(n: int, cell: np.ndarray, t_rod: float, t_amb: float):
     return fixed, tfix
 
 
+def build_spec(particles, mat: Material, heater, grid: GridConfig, spacing: float, t_init: float, kappa_air: float,
+               heat_tol: float = 1e-6, heat_maxiter: int = 200):
+    """Host-side scene construction of solver.py:42-61 (no device work): masks, fixed cells, statics, parameters.
+    Returns (SceneSpec, cell classes, heater geometry, t_max)."""
+    n, h = grid_edge(grid), grid.h
+    cell, solid, source, rate, k_faces, m_faces, geom = heater.masks(n, h, (grid.L / 2, grid.L / 2), grid.rho)
+    fixed, tfix = wall_fixed(n, cell, heater.t_rod, grid.t_amb)
+    t_max = max(heater.t_rod, heater.t_cap, grid.t_amb, t_init)
+    spec = SceneSpec(n=n, h=h, rho=grid.rho, t_amb=grid.t_amb, alpha_f_min=grid.alpha_f_min, buoyancy=grid.buoyancy,
+                     cg_tol=grid.cg_tol, cg_max_iter=grid.cg_max_iter, heat_tol=heat_tol, heat_maxiter=heat_maxiter,
+                     kappa_air=kappa_air, kappa_mat=mat.kappa, fixed=fixed, tfix=tfix, source=source, rate=rate,
+                     t_cap=heater.t_cap, static_alpha=solid.astype(np.float32), static_k=k_faces, static_m=m_faces,
+                     n_particles=len(particles), spacing=spacing, k_particle=K_PARTICLE, t_sol=mat.t_sol,
+                     t_liq=mat.t_liq, y_solid=mat.yield_solid, mu_s=mat.viscosity_solid, mu_l=mat.viscosity_liquid,
+                     t_max=t_max)
+    return spec, cell, geom, t_max
+
+
 class HeatflowMPM:
     def __init__(self, particles: np.ndarray, mat: Material = Material(), heater: Heater = Heater(),
                  grid: GridConfig = GridConfig(), spacing: float = 2.5e-3, t_init: float = 20.0,
@@ -42,27 +60,18 @@ class HeatflowMPM:
             raise RuntimeError("HeatflowMPM needs a CUDA device (sm_100a); there is no CPU path")
         self.mat, self.heater, self.dev, self.spacing, self.kappa_air = mat, heater, device, spacing, kappa_air
         self.grid = AirGrid(grid, device)
-        n, h = self.grid.n, self.grid.h
-        self.heat = HeatField(n, h, grid.t_amb, device)
-        cell, solid, source, rate, k_faces, m_faces, self.heater_geom = heater.masks(n, h, (grid.L / 2, grid.L / 2), grid.rho)
-        self.cell_type = cell
-        fixed, tfix = wall_fixed(n, cell, heater.t_rod, grid.t_amb)
-        self.t_max = max(heater.t_rod, heater.t_cap, grid.t_amb, t_init)
+        self.heat = HeatField(self.grid.n, self.grid.h, grid.t_amb, device)
         particles = np.zeros((0, 3), np.float32) if particles is None else np.asarray(particles, np.float32)
         self.n = len(particles)
-        spec = SceneSpec(n=n, h=h, rho=grid.rho, t_amb=grid.t_amb, alpha_f_min=grid.alpha_f_min, buoyancy=grid.buoyancy,
-                         cg_tol=grid.cg_tol, cg_max_iter=grid.cg_max_iter, heat_tol=heat_tol, heat_maxiter=heat_maxiter,
-                         kappa_air=kappa_air, kappa_mat=mat.kappa, fixed=fixed, tfix=tfix, source=source, rate=rate,
-                         t_cap=heater.t_cap, static_alpha=solid.astype(np.float32), static_k=k_faces, static_m=m_faces,
-                         n_particles=self.n, spacing=spacing, k_particle=K_PARTICLE, t_sol=mat.t_sol, t_liq=mat.t_liq,
-                         y_solid=mat.yield_solid, mu_s=mat.viscosity_solid, mu_l=mat.viscosity_liquid, t_max=self.t_max)
+        spec, self.cell_type, self.heater_geom, self.t_max = build_spec(particles, mat, heater, grid, spacing, t_init,
+                                                                        kappa_air, heat_tol, heat_maxiter)
         with torch.cuda.device(torch.device(device)):
             self.scene = DeviceScene(spec, device)
             self.plan = ScenePlan([self.scene], device, persistent_blocks=persistent_blocks)
             self.plan.prepare_statics()
         self.grid._bind(self.scene, self.plan, 0)
         self.heat._bind(self.scene)
-        self.grid.set_static(solid.astype(np.float32), k_faces, m_faces)
+        self.grid.set_static(spec.static_alpha, spec.static_k, spec.static_m)
         if self.n:
             if body == "frozen":
                 self.body = FrozenBody(particles, spacing, mat, device, particle_velocities)
@@ -113,7 +122,12 @@ class HeatflowMPM:
     def melt_fraction(self):
         return self.scene.pmelt.cpu().numpy()[: self.n] if self.n else np.zeros(0, np.float32)
 
-    def grid_T(self):
+    def grid_T(self, out=None):
+        """solver.py:95: grid temperature (n,n,n) on the host.  `out` (optional, e.g. a pinned torch tensor) receives
+        the copy instead of a new numpy array."""
+        if out is not None:
+            out.copy_(self.heat.T)
+            return out
         return self.heat.T.cpu().numpy()
 
     def air_velocity(self):

@@ -144,6 +144,10 @@ int hf_face_stage(const hf_plan *plan, double dt, void *stream);
  * grid.py:239), k_jacobi, warp.optim.linear.cg(k_laplacian, check_every=20) warm-started from p, k_project x3; then
  * flips every scene's parity (end of substep) */
 int hf_pressure_solve(const hf_plan *plan, double dt, void *stream);
+/* the two launches of hf_pressure_solve, separately (grid.py:237 k_divergence_rhs + per-chunk sums for the mean;
+ * grid.py:238-251 mean removal, k_jacobi, CG, k_project and the end of the substep) */
+int hf_divergence_stage(const hf_plan *plan, double dt, void *stream);
+int hf_pressure_cg(const hf_plan *plan, double dt, void *stream);
 /* the whole air substep in order (solver.py:63-88 minus the MPM step) */
 int hf_substep(const hf_plan *plan, double dt, void *stream);
 

@@ -231,6 +231,18 @@ class OracleScene:
                     viscosity=self.a["pvisc"][:P])
 
 
+def scene_from_spec(spec, precision="f32", mean_mode=0, scatter_mode=0, particles=None, pvel=None, ptemp=None):
+    """OracleScene with the parameters of a heatflow_mpm SceneSpec (any object with the same attribute names)."""
+    return OracleScene(spec.n, spec.h, precision=precision, rho=spec.rho, t_amb=spec.t_amb, alpha_f_min=spec.alpha_f_min,
+                       cg_tol=spec.cg_tol, cg_max_iter=spec.cg_max_iter, buoyancy=spec.buoyancy, kappa_air=spec.kappa_air,
+                       kappa_mat=spec.kappa_mat, g=spec.g, heat_tol=spec.heat_tol, heat_maxiter=spec.heat_maxiter,
+                       mean_mode=mean_mode, scatter_mode=scatter_mode, fixed=spec.fixed, tfix=spec.tfix, src=spec.source,
+                       rate=spec.rate, t_cap=spec.t_cap, static_alpha=spec.static_alpha, static_k=spec.static_k,
+                       static_m=spec.static_m, particles=particles, pvel=pvel, ptemp=ptemp, spacing=spec.spacing,
+                       k_particle=spec.k_particle, t_sol=spec.t_sol, t_liq=spec.t_liq, y_solid=spec.y_solid,
+                       mu_s=spec.mu_s, mu_l=spec.mu_l, t_max=spec.t_max)
+
+
 def scene_from_fixture(fx, precision="f32", mean_mode=1, scatter_mode=1):
     """Build an OracleScene from a tests/golden/substep_*.npz fixture (the reference's own inputs)."""
     n = int(fx["n"])

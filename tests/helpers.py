@@ -66,12 +66,4 @@ def random_scene_inputs(n, seed, heater_kw=None, L=None, particles=0):
 
 def oracle_from_spec(spec, precision="f32", mean_mode=0, scatter_mode=0, particles=None, pvel=None, ptemp=None):
     from oracle import oracle as O
-    return O.OracleScene(spec.n, spec.h, precision=precision, rho=spec.rho, t_amb=spec.t_amb,
-                         alpha_f_min=spec.alpha_f_min, cg_tol=spec.cg_tol, cg_max_iter=spec.cg_max_iter,
-                         buoyancy=spec.buoyancy, kappa_air=spec.kappa_air, kappa_mat=spec.kappa_mat, g=spec.g,
-                         heat_tol=spec.heat_tol, heat_maxiter=spec.heat_maxiter, mean_mode=mean_mode,
-                         scatter_mode=scatter_mode, fixed=spec.fixed, tfix=spec.tfix, src=spec.source, rate=spec.rate,
-                         t_cap=spec.t_cap, static_alpha=spec.static_alpha, static_k=spec.static_k,
-                         static_m=spec.static_m, particles=particles, pvel=pvel, ptemp=ptemp, spacing=spec.spacing,
-                         k_particle=spec.k_particle, t_sol=spec.t_sol, t_liq=spec.t_liq, y_solid=spec.y_solid,
-                         mu_s=spec.mu_s, mu_l=spec.mu_l, t_max=spec.t_max)
+    return O.scene_from_spec(spec, precision, mean_mode, scatter_mode, particles, pvel, ptemp)
