@@ -36,8 +36,11 @@ struct DeviceInfo {
     int sms = 0;
     int coop = 0;
     int occ_heat = 0, occ_pressure = 0;
+    int occ_res[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};   // [heat][maxc]: blocks/SM at the variant's block size
     bool ready = false;
 };
+
+constexpr int kResGroupsMax[4] = {0, 4, 3, 2};   // 256-thread groups per block of the resident variant, by MAXC
 
 std::mutex g_mu;
 DeviceInfo g_dev[64];
@@ -57,6 +60,11 @@ int device_info(DeviceInfo** out) {
         HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_heat, hf::pcg_kernel(true), hf::kThreads, 0), "occupancy");
         HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_pressure, hf::pcg_kernel(false), hf::kThreads, 0),
                 "occupancy");
+        for (int h = 0; h < 2; ++h)
+            for (int m = 1; m <= 3; ++m)
+                HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_res[h][m], hf::pcg_resident_kernel(h == 1, m),
+                                                                      256 * kResGroupsMax[m], 0),
+                        "occupancy (resident)");
         if (!d.coop) return fail(HF_ERR_DEVICE, "device does not support cooperative launches");
         d.ready = true;
     }
@@ -125,6 +133,26 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
     int rc = device_info(&d);
     if (rc) return rc;
     if (p->num_chunks == 0) return HF_OK;
+    hf::Workspace ws = workspace(p);
+    const hf_scene* scenes = static_cast<const hf_scene*>(p->scenes_dev);
+    const hf::WorkItem* work = static_cast<const hf::WorkItem*>(p->work_dev);
+    int nc = p->num_chunks, ns = p->num_scenes;
+    void* args[] = {(void*)&scenes, (void*)&work, (void*)&nc, (void*)&ns, (void*)&dt, (void*)&ws};
+    // register-resident variant: one active scene whose chunks fit one block per SM
+    int active = 0;
+    for (int s = 0; s < p->num_scenes; ++s) active += (p->scenes_host[s].flags & HF_FLAG_ACTIVE) ? 1 : 0;
+    if (active == 1 && !(p->options & HF_PLAN_STREAMING_CG)) {
+        const int G = p->num_chunks < d->sms ? p->num_chunks : d->sms;
+        const int cpb = (p->num_chunks + G - 1) / G;
+        for (int m = 1; m <= 3; ++m) {
+            const int groups = (cpb + m - 1) / m;
+            if (groups > kResGroupsMax[m] || d->occ_res[heat ? 1 : 0][m] < 1) continue;
+            HF_CUDA(cudaMemsetAsync(ws.bar, 0, 64, S(stream)), "cudaMemsetAsync(barrier)");
+            HF_CUDA(cudaLaunchCooperativeKernel(hf::pcg_resident_kernel(heat, m), dim3(G), dim3(256 * groups), args, 0, S(stream)),
+                    "cooperative launch (resident CG)");
+            return HF_OK;
+        }
+    }
     const int occ = heat ? d->occ_heat : d->occ_pressure;
     if (occ <= 0) return fail(HF_ERR_DEVICE, "persistent CG kernel does not fit on an SM");
     int per_sm = occ < 2 ? occ : 2;
@@ -145,13 +173,8 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
         const int s1 = (int)(std::upper_bound(begin.begin(), begin.end(), c1 - 1) - begin.begin()) - 1;
         if (s1 - s0 + 1 > 32) return fail(HF_ERR_ARG, "more than 32 scenes in one block's chunk range: use more blocks");
     }
-    hf::Workspace ws = workspace(p);
     // barrier counters, live counts and the timeout flag start at zero for every solve
     HF_CUDA(cudaMemsetAsync(ws.bar, 0, 64, S(stream)), "cudaMemsetAsync(barrier)");
-    const hf_scene* scenes = static_cast<const hf_scene*>(p->scenes_dev);
-    const hf::WorkItem* work = static_cast<const hf::WorkItem*>(p->work_dev);
-    int nc = p->num_chunks, ns = p->num_scenes;
-    void* args[] = {(void*)&scenes, (void*)&work, (void*)&nc, (void*)&ns, (void*)&dt, (void*)&ws};
     const void* fn = hf::pcg_kernel(heat);
     HF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(hf::kThreads), args, 0, S(stream)), "cooperative launch (CG)");
     return HF_OK;
@@ -217,6 +240,7 @@ int hf_obstacle_fields(const hf_plan* p, int all_scenes, void* stream) {
         const hf_scene& sc = p->scenes_host[s];
         if (!(sc.flags & HF_FLAG_ACTIVE) || !(sc.flags & HF_FLAG_PARTICLES) || sc.n_particles <= 0) continue;
         if (!sc.acc || !sc.pos || !sc.pvel || !sc.ptemp) return fail(HF_ERR_ARG, "coupled scene without particle buffers");
+        hf::k_footprint<<<(sc.n_particles + hf::kThreads - 1) / hf::kThreads, hf::kThreads, 0, S(stream)>>>(scenes, s);
         hf::k_scatter<<<(sc.n_particles + hf::kThreads - 1) / hf::kThreads, hf::kThreads, 0, S(stream)>>>(scenes, s);
     }
     if (p->num_chunks) {

@@ -107,24 +107,38 @@ __device__ __forceinline__ float lap_acc(const hf_scene& S, const X& x, float xc
     return acc;
 }
 
-// heat.py:55-91 neighbour_terms with use_fixed = 0
+// heat.py:55-91 neighbour_terms with use_fixed = 0; kappa_f from the precomputed face diffusivities
 template <class X>
 __device__ __forceinline__ float heat_nt(const hf_scene& S, const X& x, float xc, int t, int i, int j, int k) {
     const int n = S.n, nn = n * n;
-    const float* __restrict__ kap = S.kap;
     const uint8_t* __restrict__ fl = S.cell_flags;
-    const float kc = __ldg(kap + t);
     float acc = 0.0f;
     const int nbr[6] = {t - nn, t + nn, t - n, t + n, t - 1, t + 1};
     const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
+    const int fidx[6] = {uidx_(n, i, j, k), uidx_(n, i + 1, j, k), vidx_(n, i, j, k), vidx_(n, i, j + 1, k),
+                         widx_(n, i, j, k), widx_(n, i, j, k + 1)};
+    const float* __restrict__ hk[3] = {S.hkx, S.hky, S.hkz};
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
         if (!in[s]) continue;
         const int nb = nbr[s];
-        const float kf = face_kappa(kc, kap[nb]);
-        acc = __fadd_rn(acc, (fl[nb] & 1) ? __fmul_rn(kf, xc) : __fmul_rn(kf, __fsub_rn(xc, x(nb))));
+        const float kf = __ldg(hk[s >> 1] + fidx[s]);
+        acc = __fadd_rn(acc, (__ldg(fl + nb) & 1) ? __fmul_rn(kf, xc) : __fmul_rn(kf, __fsub_rn(xc, x(nb))));
     }
     return acc;
+}
+
+// heat.py:121-144 k_heat_diag: sum of the in-domain face diffusivities
+__device__ __forceinline__ float heat_diag_sum(const hf_scene& S, int i, int j, int k) {
+    const int n = S.n;
+    float s = 0.0f;
+    if (i > 0) s = __fadd_rn(s, S.hkx[uidx_(n, i, j, k)]);
+    if (i < n - 1) s = __fadd_rn(s, S.hkx[uidx_(n, i + 1, j, k)]);
+    if (j > 0) s = __fadd_rn(s, S.hky[vidx_(n, i, j, k)]);
+    if (j < n - 1) s = __fadd_rn(s, S.hky[vidx_(n, i, j + 1, k)]);
+    if (k > 0) s = __fadd_rn(s, S.hkz[widx_(n, i, j, k)]);
+    if (k < n - 1) s = __fadd_rn(s, S.hkz[widx_(n, i, j, k + 1)]);
+    return s;
 }
 
 constexpr int kLocalScenes = 32;   // scenes one block may touch (the host checks)
@@ -193,15 +207,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
                     r = __fsub_rn(b, xc);
                 } else {
                     // heat.py:121-144 k_heat_diag
-                    const float kc = S.kap[t];
-                    float s = 0.0f;
-                    if (i > 0) s = __fadd_rn(s, face_kappa(kc, S.kap[t - n * n]));
-                    if (i < n - 1) s = __fadd_rn(s, face_kappa(kc, S.kap[t + n * n]));
-                    if (j > 0) s = __fadd_rn(s, face_kappa(kc, S.kap[t - n]));
-                    if (j < n - 1) s = __fadd_rn(s, face_kappa(kc, S.kap[t + n]));
-                    if (k > 0) s = __fadd_rn(s, face_kappa(kc, S.kap[t - 1]));
-                    if (k < n - 1) s = __fadd_rn(s, face_kappa(kc, S.kap[t + 1]));
-                    d = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(c_dt, s)));
+                    d = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(c_dt, heat_diag_sum(S, i, j, k))));
                     r = __fsub_rn(b, __fadd_rn(xc, __fmul_rn(c_dt, heat_nt(S, X, xc, t, i, j, k))));
                 }
                 S.hdiag[t] = d;
@@ -453,6 +459,357 @@ finish:
             }
         }
     }
+}
+
+// ================================================================================ register-resident variant
+// Single-scene plans whose chunks fit one block per SM keep the whole CG state of their cells in registers: every
+// thread owns the same cells for the entire solve (x, r, z, p, D and Ap never leave the SM); per iteration only the
+// search direction p (phase A) and z (phase B) are published to global memory, because neighbouring blocks read them
+// at their stencil points.  The chunk -> (group, thread) mapping and the reduction tree are those of k_pcg (256
+// virtual threads x 4 cells per chunk, warp butterfly, 8 warps in order), so both kernels produce the same bits.
+//
+// Block = `groups` x 256 threads; group g owns chunks c0 + g + groups*q (q < MAXC) of the block's contiguous range.
+template <int K>
+__device__ __forceinline__ void group_sum(double (&v)[K], double* red) {
+    // red: K * (blockDim.x / 32) doubles; every 256-thread group reduces its own 8 warps in index order
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int g0 = (warp >> 3) << 3;   // first warp of this group
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) red[c * nw + warp] = v[c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s += red[c * nw + g0 + q];
+        v[c] = s;
+    }
+}
+
+// scene_sums for blocks of any size: the first 256 threads form the same tree as scene_sums in a 256-thread block.
+template <int K>
+__device__ __forceinline__ void scene_sums_g(const double* __restrict__ buf, int b, int e, const int (&comp)[K],
+                                             double (&tot)[K], double* red) {
+#pragma unroll
+    for (int q = 0; q < K; ++q) tot[q] = 0.0;
+    if (threadIdx.x < kThreads) {
+        for (int c = b + threadIdx.x; c < e; c += kThreads) {
+#pragma unroll
+            for (int q = 0; q < K; ++q) tot[q] += buf[3 * c + comp[q]];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tot[c] += __shfl_xor_sync(0xffffffffu, tot[c], o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0 && warp < kThreads / 32) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) red[c * (kThreads / 32) + warp] = tot[c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < kThreads / 32; ++q) sum += red[c * (kThreads / 32) + q];
+        tot[c] = sum;
+    }
+}
+
+template <bool HEAT, int MAXC>
+__global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1) k_pcg_res(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+                                                    int num_chunks, int num_scenes, double dt_d, Workspace ws) {
+    constexpr int CPT = kCellsPerThread * MAXC;   // cells per thread
+    __shared__ double red[3 * 32];
+    __shared__ LocalScene Ls;
+    const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
+    const int c0 = (int)(((long long)num_chunks * blockIdx.x) / gridDim.x);
+    const int c1 = (int)(((long long)num_chunks * (blockIdx.x + 1)) / gridDim.x);
+    const int sidx = work[c0].scene;                       // one scene per plan on this path
+    const hf_scene& S = scenes[sidx];
+    const int n = S.n, N = n * n * n, nn = n * n;
+    const int par = S.state->parity;
+    unsigned* bar = ws.bar + (HEAT ? 0 : 1);
+    unsigned epoch = 0;
+    const float dt = (float)dt_d;
+    const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
+    double* bufA = ws.partials;
+    double* bufB = ws.partials + 3 * (size_t)num_chunks;
+    const int cb = ws.chunk_begin[sidx], ce = ws.chunk_begin[sidx + 1];
+    float* xg = HEAT ? S.T[par ^ 1] : S.p;
+    float* zg = S.cg_z;
+
+    // cells of this thread: chunk q, sub-cell m -> slot q*4+m (chunks of a one-scene plan are consecutive)
+    float x[CPT], r[CPT], z[CPT], p[CPT], D[CPT], Ap[CPT];
+    const int cell0 = (c0 + g - cb) * kChunk + lt;
+    const int cstep = groups * kChunk;
+    const int clim = min(N, (c1 - cb) * kChunk);
+#define TCELL(s_) (cell0 + ((s_) / kCellsPerThread) * cstep + ((s_) % kCellsPerThread) * kThreads)
+#define TVALID(t_) ((t_) < clim)
+    // ------------------------------------------------------------------ prologue (as k_pcg, values kept in regs)
+    float mean = 0.0f;
+    if (!HEAT) {
+        double mm[1];
+        const int comp[1] = {0};
+        scene_sums_g<1>(bufA, cb, ce, comp, mm, red);   
+        mean = __double2float_rn(mm[0] / ((double)n * n * n));
+    }
+    {
+        const Vec X{xg};
+#pragma unroll
+        for (int s = 0; s < CPT; ++s) {
+            x[s] = r[s] = z[s] = p[s] = D[s] = Ap[s] = 0.0f;
+            const int t = TCELL(s);
+            if (!TVALID(t)) continue;
+            int i, j, k;
+            cell_ijk(t, n, i, j, k);
+            float b, d, rr;
+            const float xc = xg[t];
+            if (HEAT) {
+                b = S.hrhs[t];
+                if (S.cell_flags[t] & 1) {
+                    d = 1.0f;
+                    rr = __fsub_rn(b, xc);
+                } else {
+                    d = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(c_dt, heat_diag_sum(S, i, j, k))));
+                    rr = __fsub_rn(b, __fadd_rn(xc, __fmul_rn(c_dt, heat_nt(S, X, xc, t, i, j, k))));
+                }
+            } else {
+                b = S.rhs[t];
+                if (mean != 0.0f) {
+                    b = __fsub_rn(b, mean);
+                    S.rhs[t] = b;
+                }
+                float sa = 0.0f;
+                if (i > 0) sa = __fadd_rn(sa, S.ax[uidx_(n, i, j, k)]);
+                if (i < n - 1) sa = __fadd_rn(sa, S.ax[uidx_(n, i + 1, j, k)]);
+                if (j > 0) sa = __fadd_rn(sa, S.ay[vidx_(n, i, j, k)]);
+                if (j < n - 1) sa = __fadd_rn(sa, S.ay[vidx_(n, i, j + 1, k)]);
+                if (k > 0) sa = __fadd_rn(sa, S.az[widx_(n, i, j, k)]);
+                if (k < n - 1) sa = __fadd_rn(sa, S.az[widx_(n, i, j, k + 1)]);
+                d = __fdiv_rn(hh, maxf_(sa, 1.0e-12f));
+                rr = __fsub_rn(b, __fdiv_rn(lap_acc(S, X, xc, t, i, j, k), hh));
+            }
+            x[s] = xc;
+            D[s] = d;
+            r[s] = rr;
+            z[s] = __fmul_rn(d, rr);
+            Ap[s] = b;   // holds b until the partial sums below
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < MAXC; ++q) {
+        double part[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int m = 0; m < kCellsPerThread; ++m) {
+            const int s = q * kCellsPerThread + m, t = TCELL(s);
+            if (!TVALID(t)) continue;
+            zg[t] = z[s];
+            part[0] += (double)Ap[s] * (double)Ap[s];
+            part[1] += (double)r[s] * (double)r[s];
+            part[2] += (double)r[s] * (double)z[s];
+        }
+        group_sum<3>(part, red);
+        const int c = c0 + g + groups * q;
+        if (lt == 0 && c < c1) {
+            bufB[3 * c] = part[0];
+            bufB[3 * c + 1] = part[1];
+            bufB[3 * c + 2] = part[2];
+        }
+    }
+    if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+    {
+        double tot[3];
+        const int comp[3] = {0, 1, 2};
+        scene_sums_g<3>(bufB, cb, ce, comp, tot, red);
+        if (threadIdx.x == 0) {
+            const double tol = HEAT ? S.heat_tol : S.cg_tol;
+            double atol = tol * sqrt(tot[0]);
+            if (atol < tol) atol = tol;
+            if (atol < 1.0e-18) atol = 1.0e-18;
+            int maxit = HEAT ? S.heat_maxiter : S.cg_max_iter;
+            if (maxit <= 0) maxit = N;
+            Ls.maxit = maxit + (maxit & 1);
+            Ls.bb = tot[0];
+            Ls.rr = tot[1];
+            Ls.rz = tot[2];
+            Ls.atol_sq = atol * atol;
+            Ls.iters = 0;
+            Ls.beta = 0.0f;
+            Ls.mean = (double)mean;
+            Ls.status = isfinite(tot[1]) ? 0 : HF_SCENE_NONFINITE;
+            Ls.live = tot[1] > Ls.atol_sq && isfinite(tot[1]) && Ls.maxit > 0;
+        }
+        __syncthreads();
+    }
+    // ------------------------------------------------------------------------------------------ iterations
+    for (int kit = 1; Ls.live; ++kit) {
+        // phase A: p_k (own cells from registers, neighbours from z and p_{k-1} in global memory), Ap, p.Ap
+        const float beta = Ls.beta;
+        const bool first = kit == 1;
+        const float* pold = S.cg_p[(kit - 1) & 1];
+        float* pnew = S.cg_p[kit & 1];
+        const Dir P{zg, pold, beta, first};
+#pragma unroll
+        for (int s = 0; s < CPT; ++s) {
+            const int t = TCELL(s);
+            if (!TVALID(t)) continue;
+            const float pc = first ? z[s] : __fadd_rn(z[s], __fmul_rn(beta, p[s]));
+            int i, j, k;
+            cell_ijk(t, n, i, j, k);
+            if (HEAT) {
+                Ap[s] = (__ldg(S.cell_flags + t) & 1) ? pc : __fadd_rn(pc, __fmul_rn(c_dt, heat_nt(S, P, pc, t, i, j, k)));
+            } else {
+                Ap[s] = __fdiv_rn(lap_acc(S, P, pc, t, i, j, k), hh);
+            }
+            p[s] = pc;
+        }
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            double part[1] = {0.0};
+#pragma unroll
+            for (int m = 0; m < kCellsPerThread; ++m) {
+                const int s = q * kCellsPerThread + m, t = TCELL(s);
+                if (!TVALID(t)) continue;
+                pnew[t] = p[s];
+                part[0] += (double)p[s] * (double)Ap[s];
+            }
+            group_sum<1>(part, red);
+            const int c = c0 + g + groups * q;
+            if (lt == 0 && c < c1) bufA[3 * c] = part[0];
+        }
+        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        {
+            double tot[1];
+            const int comp[1] = {0};
+            scene_sums_g<1>(bufA, cb, ce, comp, tot, red);
+            if (threadIdx.x == 0) {
+                Ls.pAp = tot[0];
+                Ls.alpha = __double2float_rn(Ls.rz / tot[0]);
+            }
+            __syncthreads();
+        }
+        // phase B: x += alpha p, r -= alpha Ap, z = D r (registers), publish z, r.r and r.z
+        const float alpha = Ls.alpha;
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            double part[2] = {0.0, 0.0};
+#pragma unroll
+            for (int m = 0; m < kCellsPerThread; ++m) {
+                const int s = q * kCellsPerThread + m, t = TCELL(s);
+                if (!TVALID(t)) continue;
+                x[s] = __fadd_rn(x[s], __fmul_rn(alpha, p[s]));
+                r[s] = __fsub_rn(r[s], __fmul_rn(alpha, Ap[s]));
+                z[s] = __fmul_rn(D[s], r[s]);
+                zg[t] = z[s];
+                part[0] += (double)r[s] * (double)r[s];
+                part[1] += (double)r[s] * (double)z[s];
+            }
+            group_sum<2>(part, red);
+            const int c = c0 + g + groups * q;
+            if (lt == 0 && c < c1) {
+                bufB[3 * c + 1] = part[0];
+                bufB[3 * c + 2] = part[1];
+            }
+        }
+        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        {
+            double tot[2];
+            const int comp[2] = {1, 2};
+            scene_sums_g<2>(bufB, cb, ce, comp, tot, red);
+            if (threadIdx.x == 0) {
+                const double rr = tot[0], rz = tot[1];
+                Ls.iters = kit;
+                const bool above = rr > Ls.atol_sq;
+                Ls.beta = above ? __double2float_rn(rz / Ls.rz) : 0.0f;
+                Ls.rz = rz;
+                Ls.rr = rr;
+                if (!isfinite(rr)) Ls.status |= HF_SCENE_NONFINITE;
+                const bool live = above && isfinite(rr) && kit < Ls.maxit;
+                if (!live && above && isfinite(rr)) Ls.status |= HEAT ? HF_SCENE_HEAT_MAXITER : HF_SCENE_PRESSURE_MAXITER;
+                Ls.live = live;
+            }
+            __syncthreads();
+        }
+    }
+    // ------------------------------------------------------------------ write the solution back
+#pragma unroll
+    for (int s = 0; s < CPT; ++s)
+        if (TVALID(TCELL(s))) xg[TCELL(s)] = x[s];
+    if (!HEAT) {
+        // grid.py:140-153: the projection reads p at neighbour cells owned by other blocks
+        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        const float dtr = (float)(dt_d / S.rho);
+        float *u = S.u[par ^ 1], *v = S.v[par ^ 1], *w = S.w[par ^ 1];
+        const float* pp = S.p;
+#pragma unroll
+        for (int s = 0; s < CPT; ++s) {
+            const int t = TCELL(s);
+            if (!TVALID(t)) continue;
+            int i, j, k;
+            cell_ijk(t, n, i, j, k);
+            const float pc = x[s];
+            int f = uidx_(n, i, j, k);
+            u[f] = i == 0 ? 0.0f : __fsub_rn(u[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, pp[t - nn])), h));
+            f = vidx_(n, i, j, k);
+            v[f] = j == 0 ? 0.0f : __fsub_rn(v[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, pp[t - n])), h));
+            f = widx_(n, i, j, k);
+            w[f] = k == 0 ? 0.0f : __fsub_rn(w[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, pp[t - 1])), h));
+            if (i == n - 1) u[uidx_(n, n, j, k)] = 0.0f;
+            if (j == n - 1) v[vidx_(n, i, n, k)] = 0.0f;
+            if (k == n - 1) w[widx_(n, i, j, n)] = 0.0f;
+        }
+    }
+finish:
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const bool timed_out = *(volatile int*)ws.err != 0;
+        hf_scene_state* st = S.state;
+        if (HEAT) {
+            st->status = Ls.status | (timed_out ? HF_SCENE_BARRIER_TIMEOUT : 0);
+            st->heat_iters = Ls.iters;
+            st->heat_rr = Ls.rr;
+            st->heat_atol = sqrt(Ls.atol_sq);
+            st->heat_bb = Ls.bb;
+            st->total_heat_iters += Ls.iters;
+        } else {
+            st->status |= Ls.status | (timed_out ? HF_SCENE_BARRIER_TIMEOUT : 0);
+            st->pressure_iters = Ls.iters;
+            st->pressure_rr = Ls.rr;
+            st->pressure_atol = sqrt(Ls.atol_sq);
+            st->pressure_bb = Ls.bb;
+            st->rhs_mean = Ls.mean;
+            st->total_pressure_iters += Ls.iters;
+            if (!timed_out) {
+                st->parity = par ^ 1;
+                st->substeps += 1;
+            }
+        }
+    }
+}
+
+#undef TCELL
+#undef TVALID
+
+const void* pcg_resident_kernel(bool heat, int maxc) {
+    if (heat) {
+        if (maxc == 1) return (const void*)k_pcg_res<true, 1>;
+        if (maxc == 2) return (const void*)k_pcg_res<true, 2>;
+        return (const void*)k_pcg_res<true, 3>;
+    }
+    if (maxc == 1) return (const void*)k_pcg_res<false, 1>;
+    if (maxc == 2) return (const void*)k_pcg_res<false, 2>;
+    return (const void*)k_pcg_res<false, 3>;
 }
 
 const void* pcg_kernel(bool heat) { return heat ? (const void*)k_pcg<true> : (const void*)k_pcg<false>; }

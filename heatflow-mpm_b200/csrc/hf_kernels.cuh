@@ -26,6 +26,7 @@ struct Workspace {
 };
 
 __global__ void k_scatter(const hf_scene* __restrict__ scenes, int s);
+__global__ void k_footprint(const hf_scene* __restrict__ scenes, int s);
 __global__ void k_obstacle(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, int all_scenes);
 __global__ void k_coeff(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, int all_scenes);
 __global__ void k_prestage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt);
@@ -45,5 +46,7 @@ __global__ void k_heat_matvec_plain(int n, float h, float dt, float alpha, float
 // persistent cooperative Jacobi-PCG kernel (heat = heat system, else pressure system + projection + end of substep);
 // arguments: (const hf_scene*, const WorkItem*, int num_chunks, int num_scenes, double dt, Workspace)
 const void* pcg_kernel(bool heat);
+// register-resident single-scene variant (MAXC chunks per 256-thread group: 1, 2 or 3); blockDim = 256 x groups
+const void* pcg_resident_kernel(bool heat, int maxc);
 
 }  // namespace hf

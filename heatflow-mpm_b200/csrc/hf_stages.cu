@@ -4,6 +4,8 @@
 // cells first + tid + 256*m, m = 0..3, so that warps read consecutive k (the contiguous axis) and every global access
 // is coalesced.  Face stages are organised by cell: a thread owns the three low faces u(i,j,k), v(i,j,k), w(i,j,k)
 // of its cell and, on the last layer, the high wall face.
+#include <climits>
+
 #include "hf_device.cuh"
 #include "hf_kernels.cuh"
 
@@ -71,6 +73,42 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const hf_scene* __restrict
     scatter_fx(acc + 11 * M, px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n, __fmul_rn(frac, S.ptemp[t]));
 }
 
+// Cells whose obstacle fields a particle can touch: floor(x/h) - 1 .. floor(x/h) + 1 per axis covers the cell lattice
+// (offset 1/2) and the face lattices (offset 0 or 1/2), the high wall face included (it belongs to cell n-1).
+__device__ __forceinline__ void footprint(float x, float h, int n, int& lo, int& hi) {
+    const int c = (int)floorf(__fdiv_rn(x, h));
+    lo = clampi(c - 1, 0, n - 1);
+    hi = clampi(c + 1, 0, n - 1);
+}
+
+__global__ void __launch_bounds__(kThreads) k_footprint(const hf_scene* __restrict__ scenes, int s) {
+    const hf_scene& S = scenes[s];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = S.n;
+    const float h = (float)S.h;
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+    if (t < S.n_particles) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) footprint(S.pos[3 * t + d], h, n, lo[d], hi[d]);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
+        hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
+    }
+    if ((threadIdx.x & 31) == 0 && lo[0] <= hi[0]) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            atomicMin(&S.state->box[d], lo[d]);
+            atomicMax(&S.state->box[3 + d], hi[d]);
+        }
+    }
+}
+
+__device__ __forceinline__ bool in_box(const int* b, int i, int j, int k, int grow_hi) {
+    return i >= b[0] && j >= b[1] && k >= b[2] && i <= b[3] + grow_hi && j <= b[4] + grow_hi && k <= b[5] + grow_hi;
+}
+
 // Obstacle fields of one substep (grid.py:202-213 plus the particle sums): reads and clears the fixed-point
 // accumulators, adds the static heater fields, zeroes the wall fluxes (grid.py:62-67).
 __device__ __forceinline__ float take(long long* acc, int idx) {
@@ -92,11 +130,15 @@ __global__ void __launch_bounds__(kThreads) k_obstacle(const hf_scene* __restric
     const int n = S.n, N = n * n * n;
     const long long M = (long long)(n + 1) * (n + 1) * (n + 1);
     long long* acc = S.acc;
+    const int* bnow = S.state->box;
+    const int* bprev = S.state->box_prev;
     for (int m = 0; m < kCellsPerThread; ++m) {
         const int t = wi.first + threadIdx.x + m * kThreads;
         if (t >= N) break;
         int i, j, k;
         cell_ijk(t, n, i, j, k);
+        // only the particles' footprint of this and the previous substep changes (the rest holds the static fields)
+        if (!all_scenes && !in_box(bnow, i, j, k, 0) && !in_box(bprev, i, j, k, 0)) continue;
         // cell lattices: alpha_s (+ static), alpha and tsum of the heat field
         float a_s = particles ? take(acc, t) : 0.0f;
         S.alpha_s[t] = plus_static(a_s, S.st_alpha, t);
@@ -131,7 +173,14 @@ __global__ void __launch_bounds__(kThreads) k_obstacle(const hf_scene* __restric
     }
 }
 
-// grid.py:46-59 (k_face_fraction) and heat.py:44-47 (k_conductivity) from the obstacle fields.
+// grid.py:46-59 (k_face_fraction) and heat.py:44-47 (k_conductivity) from the obstacle fields, plus the harmonic face
+// diffusivity of every interior face (heat.py:50-52; the same value from either side, bit for bit).  The conductivity
+// of the lower neighbour is recomputed from its alpha_s (a pure function of it) instead of read, so no cell waits on
+// another thread.  Coupled scenes rebuild only their particle footprint grown by one cell on the high side.
+__device__ __forceinline__ float conductivity(float a, float ka, float km) {
+    return __fadd_rn(ka, __fmul_rn(__fsub_rn(km, ka), clampf_(__fdiv_rn(a, 0.6f), 0.0f, 1.0f)));
+}
+
 __global__ void __launch_bounds__(kThreads) k_coeff(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
                                                    int all_scenes) {
     const WorkItem wi = work[blockIdx.x];
@@ -140,19 +189,45 @@ __global__ void __launch_bounds__(kThreads) k_coeff(const hf_scene* __restrict__
     const int n = S.n, N = n * n * n;
     const float afmin = (float)S.alpha_f_min, ka = (float)S.kappa_air, km = (float)S.kappa_mat;
     const float* as = S.alpha_s;
+    const int* bnow = S.state->box;
+    const int* bprev = S.state->box_prev;
     for (int m = 0; m < kCellsPerThread; ++m) {
         const int t = wi.first + threadIdx.x + m * kThreads;
         if (t >= N) break;
         int i, j, k;
         cell_ijk(t, n, i, j, k);
+        if (!all_scenes && !in_box(bnow, i, j, k, 1) && !in_box(bprev, i, j, k, 1)) continue;
         const float ac = as[t];
-        S.kap[t] = __fadd_rn(ka, __fmul_rn(__fsub_rn(km, ka), clampf_(__fdiv_rn(ac, 0.6f), 0.0f, 1.0f)));
-        S.ax[uidx(n, i, j, k)] = i == 0 ? 0.0f : clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(as[t - n * n], ac))), afmin, 1.0f);
-        S.ay[vidx(n, i, j, k)] = j == 0 ? 0.0f : clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(as[t - n], ac))), afmin, 1.0f);
-        S.az[widx(n, i, j, k)] = k == 0 ? 0.0f : clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(as[t - 1], ac))), afmin, 1.0f);
-        if (i == n - 1) S.ax[uidx(n, n, j, k)] = 0.0f;
-        if (j == n - 1) S.ay[vidx(n, i, n, k)] = 0.0f;
-        if (k == n - 1) S.az[widx(n, i, j, n)] = 0.0f;
+        const float kc = conductivity(ac, ka, km);
+        S.kap[t] = kc;
+        const int fu = uidx(n, i, j, k), fv = vidx(n, i, j, k), fw = widx(n, i, j, k);
+        if (i == 0) {
+            S.ax[fu] = 0.0f;
+            S.hkx[fu] = 0.0f;
+        } else {
+            const float an = as[t - n * n];
+            S.ax[fu] = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
+            S.hkx[fu] = face_kappa(conductivity(an, ka, km), kc);
+        }
+        if (j == 0) {
+            S.ay[fv] = 0.0f;
+            S.hky[fv] = 0.0f;
+        } else {
+            const float an = as[t - n];
+            S.ay[fv] = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
+            S.hky[fv] = face_kappa(conductivity(an, ka, km), kc);
+        }
+        if (k == 0) {
+            S.az[fw] = 0.0f;
+            S.hkz[fw] = 0.0f;
+        } else {
+            const float an = as[t - 1];
+            S.az[fw] = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
+            S.hkz[fw] = face_kappa(conductivity(an, ka, km), kc);
+        }
+        if (i == n - 1) S.ax[uidx(n, n, j, k)] = S.hkx[uidx(n, n, j, k)] = 0.0f;
+        if (j == n - 1) S.ay[vidx(n, i, n, k)] = S.hky[vidx(n, i, n, k)] = 0.0f;
+        if (k == n - 1) S.az[widx(n, i, j, n)] = S.hkz[widx(n, i, j, n)] = 0.0f;
     }
 }
 
@@ -220,15 +295,17 @@ __global__ void __launch_bounds__(kThreads) k_advect_T(const hf_scene* __restric
         if (fl[t] & 1) {
             rhs = S.tfix[t];
         } else {
-            const float kc = kap[t];
             float acc = 0.0f;
             const int nbr[6] = {t - n * n, t + n * n, t - n, t + n, t - 1, t + 1};
             const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
+            const float kf[6] = {in[0] ? S.hkx[uidx(n, i, j, k)] : 0.0f, in[1] ? S.hkx[uidx(n, i + 1, j, k)] : 0.0f,
+                                 in[2] ? S.hky[vidx(n, i, j, k)] : 0.0f, in[3] ? S.hky[vidx(n, i, j + 1, k)] : 0.0f,
+                                 in[4] ? S.hkz[widx(n, i, j, k)] : 0.0f, in[5] ? S.hkz[widx(n, i, j, k + 1)] : 0.0f};
 #pragma unroll
             for (int s = 0; s < 6; ++s) {
                 if (!in[s]) continue;
                 const int nb = nbr[s];
-                if (fl[nb] & 1) acc = __fadd_rn(acc, __fmul_rn(face_kappa(kc, kap[nb]), S.tfix[nb]));
+                if (fl[nb] & 1) acc = __fadd_rn(acc, __fmul_rn(kf[s], S.tfix[nb]));
             }
             rhs = __fadd_rn(out, __fmul_rn(c_dt, acc));
         }
@@ -240,6 +317,17 @@ __global__ void __launch_bounds__(kThreads) k_advect_T(const hf_scene* __restric
 __global__ void __launch_bounds__(kThreads) k_particle_update(const hf_scene* __restrict__ scenes, int s) {
     const hf_scene& S = scenes[s];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) {
+        // the footprint of this substep becomes the previous one; the next scatter starts from an empty box
+        hf_scene_state* st = S.state;
+#pragma unroll
+        for (int d = 0; d < 6; ++d) st->box_prev[d] = st->box[d];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            st->box[d] = INT_MAX;
+            st->box[3 + d] = INT_MIN;
+        }
+    }
     if (t >= S.n_particles) return;
     const int n = S.n, par = S.state->parity;
     const float h = (float)S.h;

@@ -15,6 +15,7 @@ HF_OK, HF_ERR_ARG, HF_ERR_CUDA, HF_ERR_WORKSPACE, HF_ERR_DEVICE = 0, 1, 2, 3, 4
 HF_FLAG_BUOYANCY, HF_FLAG_SOURCE, HF_FLAG_PARTICLES, HF_FLAG_ACTIVE = 1, 2, 4, 8
 HF_SCENE_HEAT_MAXITER, HF_SCENE_PRESSURE_MAXITER, HF_SCENE_NONFINITE, HF_SCENE_BARRIER_TIMEOUT = 1, 2, 4, 8
 CHUNK = 1024
+HF_PLAN_STREAMING_CG = 1
 
 _P = C.c_void_p
 
@@ -25,7 +26,7 @@ class SceneState(C.Structure):
                 ("heat_rr", C.c_double), ("heat_atol", C.c_double), ("pressure_rr", C.c_double),
                 ("pressure_atol", C.c_double), ("pressure_bb", C.c_double), ("heat_bb", C.c_double),
                 ("rhs_mean", C.c_double), ("total_heat_iters", C.c_int64), ("total_pressure_iters", C.c_int64),
-                ("reserved", C.c_double * 4)]
+                ("box", C.c_int32 * 6), ("box_prev", C.c_int32 * 6), ("reserved_box", C.c_int32 * 4)]
 
 
 SCENE_DOUBLES = ("h", "rho", "t_amb", "alpha_f_min", "g", "cg_tol", "heat_tol", "kappa_air", "kappa_mat", "rate",
@@ -43,13 +44,13 @@ class Scene(C.Structure):
                [(f, _P) for f in SCENE_PTRS[:31]] + \
                [("cg_r", _P), ("cg_z", _P), ("cg_p", _P * 2), ("cg_Ap", _P),
                 ("pos", _P), ("pvel", _P), ("ptemp", _P), ("pmelt", _P), ("pyield", _P), ("pvisc", _P),
-                ("acc", _P), ("state", _P)]
+                ("hkx", _P), ("hky", _P), ("hkz", _P), ("acc", _P), ("state", _P)]
 
 
 class Plan(C.Structure):
     _fields_ = [("num_scenes", C.c_int32), ("num_chunks", C.c_int32), ("scenes_host", _P), ("scenes_dev", _P),
                 ("work_dev", _P), ("workspace", _P), ("workspace_bytes", C.c_size_t), ("persistent_blocks", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("options", C.c_int32)]
 
 
 _lib = None

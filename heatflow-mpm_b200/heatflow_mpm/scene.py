@@ -81,6 +81,7 @@ class DeviceScene:
             setattr(self, name, z(n, n, n))
         self.cg_p = [z(n, n, n), z(n, n, n)]
         self.ax, self.ay, self.az = (z(*s) for s in fs)
+        self.hk = [z(*s) for s in fs]
         self.cell_flags = z(n, n, n, dtype=torch.uint8)
         coupled = spec.n_particles > 0
         has_static = spec.static_alpha is not None
@@ -112,7 +113,11 @@ class DeviceScene:
             self.alpha, self.tsum = self.zero_cell, self.zero_cell
             self.acc = None
             self.pos = self.pvel = self.ptemp = self.pmelt = self.pyield = self.pvisc = None
-        self.state = torch.zeros(C.sizeof(_lib.SceneState), dtype=torch.uint8, device=dev)
+        st0 = _lib.SceneState()
+        for i in range(3):
+            st0.box[i] = st0.box_prev[i] = 2 ** 31 - 1
+            st0.box[3 + i] = st0.box_prev[3 + i] = -2 ** 31
+        self.state = torch.frombuffer(bytearray(bytes(st0)), dtype=torch.uint8).to(dev)
         self._parity_host = 0
         self.dirty = False
         fixed = np.zeros((n, n, n), bool) if spec.fixed is None else np.asarray(spec.fixed, bool)
@@ -182,6 +187,7 @@ class DeviceScene:
         r.st_mx, r.st_my, r.st_mz = (P(a) for a in s.st_m)
         r.cg_p[0], r.cg_p[1] = P(s.cg_p[0]), P(s.cg_p[1])
         r.pos, r.pvel, r.ptemp, r.pmelt, r.pyield, r.pvisc = (P(a) for a in (s.pos, s.pvel, s.ptemp, s.pmelt, s.pyield, s.pvisc))
+        r.hkx, r.hky, r.hkz = (P(a) for a in s.hk)
         r.acc = P(s.acc)
         r.state = P(s.state)
 
@@ -206,7 +212,7 @@ class DeviceScene:
 class ScenePlan:
     """Scene table + work table + workspace for a list of DeviceScene, and the stage calls over them."""
 
-    def __init__(self, scenes, device="cuda:0", persistent_blocks=0):
+    def __init__(self, scenes, device="cuda:0", persistent_blocks=0, streaming_cg=False):
         self.L = _lib.load()
         self.scenes = list(scenes)
         self.device = torch.device(device)
@@ -227,6 +233,7 @@ class ScenePlan:
         self.plan.workspace = self.workspace.data_ptr()
         self.plan.workspace_bytes = ws_bytes
         self.plan.persistent_blocks = persistent_blocks
+        self.plan.options = _lib.HF_PLAN_STREAMING_CG if streaming_cg else 0
         self.upload()
 
     def stream(self):

@@ -60,7 +60,12 @@ typedef struct hf_scene_state {
     double pressure_bb, heat_bb;     /* b.b of the last solves (||r||/||b|| = sqrt(rr/bb)) */
     double rhs_mean;                 /* mean removed from the pressure rhs (grid.py:238-241) */
     int64_t total_heat_iters, total_pressure_iters;
-    double reserved[4];
+    /* Particle footprint (cells, inclusive, lo i,j,k then hi i,j,k) of the current and the previous substep: the
+     * obstacle fields are rebuilt only inside their union.  An empty box has lo > hi; initialise both to empty
+     * (lo = INT32_MAX, hi = INT32_MIN) before the first substep. */
+    int32_t box[6];
+    int32_t box_prev[6];
+    int32_t reserved_box[4];
 } hf_scene_state;
 
 /* One scene: sizes, physical parameters and device pointers of its fields.  The same struct is the element of the
@@ -95,10 +100,16 @@ typedef struct hf_scene {
     float *cg_r, *cg_z, *cg_p[2], *cg_Ap;
     /* particles (P,3) / (P): positions and velocities in, temperature/melt/yield/viscosity in-out */
     float *pos, *pvel, *ptemp, *pmelt, *pyield, *pvisc;
+    /* harmonic face diffusivities 2 k_a k_b / (k_a + k_b + 1e-12) of the three face lattices (heat.py:50-52) */
+    float *hkx, *hky, *hkz;
     /* 12 fixed-point accumulators of (n+1)^3 int64 each (coupled scenes only), zero on entry, left zero */
     long long *acc;
     hf_scene_state *state;
 } hf_scene;
+
+/* hf_plan.options */
+#define HF_PLAN_STREAMING_CG 1u      /* never use the register-resident CG variant (single-scene plans use it when
+                                        the scene's chunks fit one block per SM) */
 
 /* A batch of scenes ready to launch: tables in device memory plus the host copy used to size launches. */
 typedef struct hf_plan {
@@ -110,7 +121,7 @@ typedef struct hf_plan {
     void *workspace;           /* device: >= hf_workspace_bytes(num_scenes, num_chunks) bytes */
     size_t workspace_bytes;
     int32_t persistent_blocks; /* grid of the persistent CG kernels (0 = choose: SMs x occupancy) */
-    int32_t reserved;
+    int32_t options;           /* HF_PLAN_* bits */
 } hf_plan;
 
 /* ---------------------------------------------------------------------------------------------------- set-up */
