@@ -4,6 +4,7 @@
 // memory; the workspace layout below carves the caller's buffer.
 #include <algorithm>
 #include <cstdio>
+#include <cudaTypedefs.h>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -36,7 +37,7 @@ struct DeviceInfo {
     int sms = 0;
     int coop = 0;
     int occ_heat = 0, occ_pressure = 0;
-    int occ_res[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};   // [heat][maxc]: blocks/SM at the variant's block size
+    size_t smem_optin = 0;
     bool ready = false;
 };
 
@@ -60,11 +61,9 @@ int device_info(DeviceInfo** out) {
         HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_heat, hf::pcg_kernel(true), hf::kThreads, 0), "occupancy");
         HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_pressure, hf::pcg_kernel(false), hf::kThreads, 0),
                 "occupancy");
-        for (int h = 0; h < 2; ++h)
-            for (int m = 1; m <= 3; ++m)
-                HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_res[h][m], hf::pcg_resident_kernel(h == 1, m),
-                                                                      256 * kResGroupsMax[m], 0),
-                        "occupancy (resident)");
+        int optin = 0;
+        HF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "cudaDeviceGetAttribute");
+        d.smem_optin = (size_t)optin;
         if (!d.coop) return fail(HF_ERR_DEVICE, "device does not support cooperative launches");
         d.ready = true;
     }
@@ -75,47 +74,74 @@ int device_info(DeviceInfo** out) {
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
-    size_t head, chunk_begin, ctl, scene_count, partials, diag, total;
+    size_t head, chunk_begin, tile_begin, ctl, partA, partB, mean_part, total;
 };
 
-Layout layout(int S, int C) {
+Layout layout(int S, int C, int T) {
     Layout L{};
     size_t o = 0;
     L.head = o;                      // bar[2], live_count[2], err, pad -> 64 bytes
     o = align_up(o + 64, 256);
     L.chunk_begin = o;
     o = align_up(o + sizeof(int) * (size_t)(S + 1), 256);
+    L.tile_begin = o;
+    o = align_up(o + sizeof(int) * (size_t)(S + 1), 256);
     L.ctl = o;
     o = align_up(o + sizeof(hf::CgCtl) * (size_t)S, 256);
-    L.scene_count = o;
-    o = align_up(o + sizeof(unsigned) * (size_t)S, 256);
-    L.partials = o;
-    o = align_up(o + sizeof(double) * 6 * (size_t)C, 256);   // two partial buffers (phases A and B)
-    L.diag = o;
-    o = align_up(o + 64, 256);
+    L.partA = o;
+    o = align_up(o + sizeof(double) * 3 * (size_t)T, 256);
+    L.partB = o;
+    o = align_up(o + sizeof(double) * 3 * (size_t)T, 256);
+    L.mean_part = o;
+    o = align_up(o + sizeof(double) * (size_t)C, 256);
     L.total = o;
     return L;
 }
 
 hf::Workspace workspace(const hf_plan* p) {
-    const Layout L = layout(p->num_scenes, p->num_chunks);
+    const Layout L = layout(p->num_scenes, p->num_chunks, p->num_tiles);
     char* b = static_cast<char*>(p->workspace);
     hf::Workspace w;
     w.bar = reinterpret_cast<unsigned*>(b + L.head);
     w.live_count = w.bar + 2;
     w.err = reinterpret_cast<int*>(w.bar + 4);
     w.chunk_begin = reinterpret_cast<int*>(b + L.chunk_begin);
+    w.tile_begin = reinterpret_cast<int*>(b + L.tile_begin);
     w.ctl = reinterpret_cast<hf::CgCtl*>(b + L.ctl);
-    w.scene_count = reinterpret_cast<unsigned*>(b + L.scene_count);
-    w.partials = reinterpret_cast<double*>(b + L.partials);
-    w.diag_bits = reinterpret_cast<unsigned*>(b + L.diag);
+    w.partA = reinterpret_cast<double*>(b + L.partA);
+    w.partB = reinterpret_cast<double*>(b + L.partB);
+    w.mean_part = reinterpret_cast<double*>(b + L.mean_part);
     return w;
+}
+
+int tiles_of(int n) { return ((n + hf::kTI - 1) / hf::kTI) * ((n + hf::kTJ - 1) / hf::kTJ) * ((n + hf::kTK - 1) / hf::kTK); }
+
+// TMA descriptor of a 3-D float array (k fastest) of dims (nk, nj, ni) with a box (bk, bj, bi)
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int encode_map(CUtensorMap* m, const float* base, int nk, int nj, int ni, int bk, int bj, int bi) {
+    if (!g_encode) {
+        cudaDriverEntryPointQueryResult q;
+        HF_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", reinterpret_cast<void**>(&g_encode), cudaEnableDefault, &q),
+                "cudaGetDriverEntryPoint(cuTensorMapEncodeTiled)");
+        if (q != cudaDriverEntryPointSuccess || !g_encode) return fail(HF_ERR_DEVICE, "cuTensorMapEncodeTiled unavailable");
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)nk, (cuuint64_t)nj, (cuuint64_t)ni};
+    const cuuint64_t strides[2] = {(cuuint64_t)nk * 4u, (cuuint64_t)nk * nj * 4u};
+    const cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)bj, (cuuint32_t)bi};
+    const cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(HF_ERR_DEVICE, "cuTensorMapEncodeTiled failed");
+    return HF_OK;
 }
 
 int check_plan(const hf_plan* p) {
     if (!p || !p->scenes_host || !p->scenes_dev || !p->work_dev || !p->workspace) return fail(HF_ERR_ARG, "incomplete hf_plan");
     if (p->num_scenes <= 0 || p->num_scenes > hf::kMaxScenes) return fail(HF_ERR_ARG, "num_scenes out of range (1..1024)");
-    if (p->workspace_bytes < layout(p->num_scenes, p->num_chunks).total)
+    if (!p->tiles_dev) return fail(HF_ERR_ARG, "incomplete hf_plan (tile table)");
+    if (p->workspace_bytes < layout(p->num_scenes, p->num_chunks, p->num_tiles).total)
         return fail(HF_ERR_WORKSPACE, "workspace smaller than hf_workspace_bytes()");
     return HF_OK;
 }
@@ -132,23 +158,49 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
     DeviceInfo* d = nullptr;
     int rc = device_info(&d);
     if (rc) return rc;
-    if (p->num_chunks == 0) return HF_OK;
+    if (p->num_tiles == 0) return HF_OK;
     hf::Workspace ws = workspace(p);
     const hf_scene* scenes = static_cast<const hf_scene*>(p->scenes_dev);
-    const hf::WorkItem* work = static_cast<const hf::WorkItem*>(p->work_dev);
-    int nc = p->num_chunks, ns = p->num_scenes;
-    void* args[] = {(void*)&scenes, (void*)&work, (void*)&nc, (void*)&ns, (void*)&dt, (void*)&ws};
-    // register-resident variant: one active scene whose chunks fit one block per SM
-    int active = 0;
-    for (int s = 0; s < p->num_scenes; ++s) active += (p->scenes_host[s].flags & HF_FLAG_ACTIVE) ? 1 : 0;
-    if (active == 1 && !(p->options & HF_PLAN_STREAMING_CG)) {
-        const int G = p->num_chunks < d->sms ? p->num_chunks : d->sms;
-        const int cpb = (p->num_chunks + G - 1) / G;
+    const hf::TileItem* tiles = static_cast<const hf::TileItem*>(p->tiles_dev);
+    int nt = p->num_tiles, ns = p->num_scenes;
+    // barrier counters, live counts and the timeout flag start at zero for every solve
+    HF_CUDA(cudaMemsetAsync(ws.bar, 0, 64, S(stream)), "cudaMemsetAsync(barrier)");
+    // register-resident variant: one active scene whose tiles fit one block per SM
+    int active = -1, nactive = 0;
+    for (int s = 0; s < p->num_scenes; ++s)
+        if (p->scenes_host[s].flags & HF_FLAG_ACTIVE) {
+            active = s;
+            ++nactive;
+        }
+    if (nactive == 1 && !(p->options & HF_PLAN_STREAMING_CG)) {
+        const hf_scene& sc = p->scenes_host[active];
+        const int G = p->num_tiles < d->sms ? p->num_tiles : d->sms;
+        const int tpb = (p->num_tiles + G - 1) / G;
+        const bool tma = !heat && (sc.n % 4 == 0) && !(p->options & HF_PLAN_NO_TMA);
         for (int m = 1; m <= 3; ++m) {
-            const int groups = (cpb + m - 1) / m;
-            if (groups > kResGroupsMax[m] || d->occ_res[heat ? 1 : 0][m] < 1) continue;
-            HF_CUDA(cudaMemsetAsync(ws.bar, 0, 64, S(stream)), "cudaMemsetAsync(barrier)");
-            HF_CUDA(cudaLaunchCooperativeKernel(hf::pcg_resident_kernel(heat, m), dim3(G), dim3(256 * groups), args, 0, S(stream)),
+            const int groups = (tpb + m - 1) / m;
+            if (groups > kResGroupsMax[m]) continue;
+            const void* fn = hf::pcg_resident_kernel(heat, m, tma);
+            const size_t smem = hf::pcg_resident_smem(groups, m, tma);
+            if (smem > d->smem_optin) continue;
+            if (smem > 48 * 1024)
+                HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+            int occ = 0;
+            HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256 * groups, smem), "occupancy (resident)");
+            if (occ < 1) continue;
+            hf::TileMaps maps;
+            std::memset(&maps, 0, sizeof maps);
+            if (tma) {
+                const int n = sc.n;
+                if ((rc = encode_map(&maps.z, sc.cg_z, n, n, n, 40, 10, 6))) return rc;
+                if ((rc = encode_map(&maps.p0, sc.cg_p[0], n, n, n, 40, 10, 6))) return rc;
+                if ((rc = encode_map(&maps.p1, sc.cg_p[1], n, n, n, 40, 10, 6))) return rc;
+                if ((rc = encode_map(&maps.ax, sc.ax, n, n, n + 1, 32, 8, 5))) return rc;
+                if ((rc = encode_map(&maps.ayc, sc.ayc, n, n, n, 32, 9, 4))) return rc;
+                if ((rc = encode_map(&maps.azc, sc.azc, n, n, n, 36, 8, 4))) return rc;
+            }
+            void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&nt, (void*)&ns, (void*)&dt, (void*)&ws, (void*)&maps};
+            HF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(256 * groups), args, smem, S(stream)),
                     "cooperative launch (resident CG)");
             return HF_OK;
         }
@@ -158,25 +210,24 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
     int per_sm = occ < 2 ? occ : 2;
     int grid = p->persistent_blocks > 0 ? p->persistent_blocks : d->sms * per_sm;
     if (grid > d->sms * occ) grid = d->sms * occ;
-    if (grid > p->num_chunks) grid = p->num_chunks;
-    // every block keeps the scalars of the scenes its contiguous chunk range touches (at most 32)
+    if (grid > p->num_tiles) grid = p->num_tiles;
+    // every block keeps the scalars of the scenes its contiguous tile range touches (at most 32)
     std::vector<int> begin(p->num_scenes + 1, 0);
     for (int s = 0; s < p->num_scenes; ++s) {
         const hf_scene& sc = p->scenes_host[s];
-        begin[s + 1] = begin[s] + ((sc.flags & HF_FLAG_ACTIVE) ? hf_chunks_for(sc.n) : 0);
+        begin[s + 1] = begin[s] + ((sc.flags & HF_FLAG_ACTIVE) ? tiles_of(sc.n) : 0);
     }
-    if (begin[p->num_scenes] != p->num_chunks) return fail(HF_ERR_ARG, "plan changed since hf_plan_upload");
+    if (begin[p->num_scenes] != p->num_tiles) return fail(HF_ERR_ARG, "plan changed since hf_plan_upload");
     for (int b = 0; b < grid; ++b) {
-        const int c0 = (int)(((long long)p->num_chunks * b) / grid), c1 = (int)(((long long)p->num_chunks * (b + 1)) / grid);
+        const int c0 = (int)(((long long)p->num_tiles * b) / grid), c1 = (int)(((long long)p->num_tiles * (b + 1)) / grid);
         if (c1 <= c0) continue;
         const int s0 = (int)(std::upper_bound(begin.begin(), begin.end(), c0) - begin.begin()) - 1;
         const int s1 = (int)(std::upper_bound(begin.begin(), begin.end(), c1 - 1) - begin.begin()) - 1;
-        if (s1 - s0 + 1 > 32) return fail(HF_ERR_ARG, "more than 32 scenes in one block's chunk range: use more blocks");
+        if (s1 - s0 + 1 > 32) return fail(HF_ERR_ARG, "more than 32 scenes in one block's tile range: use more blocks");
     }
-    // barrier counters, live counts and the timeout flag start at zero for every solve
-    HF_CUDA(cudaMemsetAsync(ws.bar, 0, 64, S(stream)), "cudaMemsetAsync(barrier)");
-    const void* fn = hf::pcg_kernel(heat);
-    HF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(hf::kThreads), args, 0, S(stream)), "cooperative launch (CG)");
+    void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&nt, (void*)&ns, (void*)&dt, (void*)&ws};
+    HF_CUDA(cudaLaunchCooperativeKernel(hf::pcg_kernel(heat), dim3(grid), dim3(hf::kThreads), args, 0, S(stream)),
+            "cooperative launch (CG)");
     return HF_OK;
 }
 
@@ -196,35 +247,52 @@ int hf_chunks_for(int n) {
     return (int)((N + hf::kChunk - 1) / hf::kChunk);
 }
 
-size_t hf_workspace_bytes(int num_scenes, int num_chunks) { return layout(num_scenes, num_chunks).total; }
+size_t hf_workspace_bytes(int num_scenes, int num_chunks, int num_tiles) {
+    return layout(num_scenes, num_chunks, num_tiles).total;
+}
+
+int hf_tiles_for(int n) { return n > 0 ? tiles_of(n) : 0; }
 
 int hf_plan_upload(hf_plan* p, void* stream) {
-    if (!p || !p->scenes_host || !p->scenes_dev || !p->work_dev || !p->workspace) return fail(HF_ERR_ARG, "incomplete hf_plan");
+    if (!p || !p->scenes_host || !p->scenes_dev || !p->work_dev || !p->tiles_dev || !p->workspace)
+        return fail(HF_ERR_ARG, "incomplete hf_plan");
     if (p->num_scenes <= 0 || p->num_scenes > hf::kMaxScenes) return fail(HF_ERR_ARG, "num_scenes out of range (1..1024)");
     std::vector<hf::WorkItem> work;
-    std::vector<int> begin(p->num_scenes + 1, 0);
+    std::vector<hf::TileItem> tiles;
+    std::vector<int> begin(p->num_scenes + 1, 0), tbegin(p->num_scenes + 1, 0);
     for (int s = 0; s < p->num_scenes; ++s) {
         const hf_scene& sc = p->scenes_host[s];
         begin[s] = (int)work.size();
+        tbegin[s] = (int)tiles.size();
         if (!(sc.flags & HF_FLAG_ACTIVE)) continue;
         if (sc.n < 2 || sc.n > 1024) return fail(HF_ERR_ARG, "scene edge n out of range (2..1024)");
         if (!sc.state) return fail(HF_ERR_ARG, "scene without a state block");
         const long long N = (long long)sc.n * sc.n * sc.n;
         for (long long f = 0; f < N; f += hf::kChunk) work.push_back(hf::WorkItem{s, (int)f});
+        for (int k0 = 0; k0 < sc.n; k0 += hf::kTK)
+            for (int j0 = 0; j0 < sc.n; j0 += hf::kTJ)
+                for (int i0 = 0; i0 < sc.n; i0 += hf::kTI) tiles.push_back(hf::TileItem{s, i0, j0, k0});
     }
     begin[p->num_scenes] = (int)work.size();
+    tbegin[p->num_scenes] = (int)tiles.size();
     p->num_chunks = (int)work.size();
-    const Layout L = layout(p->num_scenes, p->num_chunks);
+    p->num_tiles = (int)tiles.size();
+    const Layout L = layout(p->num_scenes, p->num_chunks, p->num_tiles);
     if (p->workspace_bytes < L.total) return fail(HF_ERR_WORKSPACE, "workspace smaller than hf_workspace_bytes()");
     HF_CUDA(cudaMemsetAsync(p->workspace, 0, L.total, S(stream)), "cudaMemsetAsync(workspace)");
     HF_CUDA(cudaMemcpyAsync(p->scenes_dev, p->scenes_host, sizeof(hf_scene) * p->num_scenes, cudaMemcpyHostToDevice, S(stream)),
             "upload scene table");
     if (!work.empty())
         HF_CUDA(cudaMemcpyAsync(p->work_dev, work.data(), sizeof(hf::WorkItem) * work.size(), cudaMemcpyHostToDevice, S(stream)),
-                "upload work table");
+                "upload chunk table");
+    if (!tiles.empty())
+        HF_CUDA(cudaMemcpyAsync(p->tiles_dev, tiles.data(), sizeof(hf::TileItem) * tiles.size(), cudaMemcpyHostToDevice, S(stream)),
+                "upload tile table");
     char* b = static_cast<char*>(p->workspace);
     HF_CUDA(cudaMemcpyAsync(b + L.chunk_begin, begin.data(), sizeof(int) * begin.size(), cudaMemcpyHostToDevice, S(stream)),
-            "upload chunk table");
+            "upload chunk offsets");
+    HF_CUDA(cudaMemcpyAsync(b + L.tile_begin, tbegin.data(), sizeof(int) * tbegin.size(), cudaMemcpyHostToDevice, S(stream)),
+            "upload tile offsets");
     HF_CUDA(cudaStreamSynchronize(S(stream)), "cudaStreamSynchronize(plan upload)");
     return HF_OK;
 }

@@ -1,42 +1,53 @@
-// hf_cg.cu -- persistent, cooperative Jacobi-preconditioned CG over a batch of scenes.
+// hf_cg.cu -- persistent, cooperative Jacobi-preconditioned CG for the heat and pressure systems of a batch of scenes.
 //
-// One launch performs a whole solve (heat.py:198-210 or grid.py:235-251) with the convergence test on the device,
-// so no iteration ever waits for the host.  The grid is co-resident (cooperative launch); phases are separated by a
-// software grid barrier whose wait is bounded in time (a timeout sets a flag and every block leaves the solve).
+// One launch performs a whole solve (heat.py:198-210 or grid.py:235-251) with the convergence test on the device, so
+// no iteration waits for the host.  The grid is co-resident (cooperative launch); phases are separated by a software
+// grid barrier whose wait is bounded in time (a timeout sets a flag and every block leaves the solve).
 //
-// Semantics follow warp.optim.linear.cg with M = diag(D) (restated from warp-lang's published algorithm; the package
-// is a dependency of the reference, not part of it):
+// Semantics follow warp.optim.linear.cg with M = diag(D) (warp-lang, a dependency of the reference; restated from its
+// published algorithm):
 //     r = b - A x,  z = D r,  p = z,  atol = max(tol ||b||, tol, 1e-18)
 //     repeat: Ap = A p; alpha = rz / pAp; x += alpha p; r -= alpha Ap; z = D r; beta = rz'/rz; p = z + beta p
 //     until r.r <= atol^2 (tested every iteration, which is where the reference's frozen iterations leave x) or maxiter.
 // Inner products, alpha and beta are fp64; the vectors stay binary32 and alpha/beta are applied after rounding.
 //
-// Two grid barriers per iteration: the search-direction update p = z + beta p is not a separate phase -- every block
-// recomputes p at the stencil points it reads (its own cells and their neighbours) from z and the previous p, which
-// are double-buffered, so the update costs no barrier.
+// Work items are 4 x 8 x 32-cell tiles (i, j, k).  Thread lt of a tile owns cells (i0 + m, j0 + lt/32, k0 + lt%32),
+// m = 0..3, so a warp covers one 128-byte k-row.  Each tile yields one fp64 partial per inner product in a fixed tree
+// (4 cells in order, warp butterfly, 8 warps in order); a scene's inner product sums its tile partials in tile order
+// (again a fixed tree).  Results therefore depend only on the scene -- not on the batch, the grid size or the variant.
 //
-// Reductions are deterministic: each 1024-cell chunk produces one fp64 partial in a fixed tree; the block that
-// completes a scene's last chunk sums that scene's partials in chunk order (again a fixed tree) and publishes the
-// scalars.  The result depends only on the scene, not on the batch it runs in or on the grid size.
+// Two grid barriers per iteration: the search direction p_k = z + beta p_{k-1} is not a separate phase -- every block
+// recomputes it at the stencil points it reads from z and the previous p (double-buffered), so it costs no barrier.
+//
+// Variants:
+//   k_pcg       streaming: vectors in global memory, any number of scenes (batched and served plans).
+//   k_pcg_res   register-resident, one scene: every thread keeps x, r, z, p, D and Ap of its cells in registers for
+//               the whole solve; only p and z are published (neighbouring blocks read them).  For the pressure system
+//               with n % 4 == 0 the stencil inputs of each tile -- z and the previous p with a one-cell halo, and the
+//               face fractions -- are staged into shared memory by TMA (cp.async.bulk.tensor) instead of gathered.
+#include <cuda.h>
+
 #include "hf_device.cuh"
 #include "hf_kernels.cuh"
 
 namespace hf {
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;   // 2 s
+constexpr int kLocalScenes = 32;                                  // scenes one streaming block may touch
 
 __device__ __forceinline__ int uidx_(int n, int i, int j, int k) { return (i * n + j) * n + k; }
 __device__ __forceinline__ int vidx_(int n, int i, int j, int k) { return (i * (n + 1) + j) * n + k; }
 __device__ __forceinline__ int widx_(int n, int i, int j, int k) { return (i * n + j) * (n + 1) + k; }
 
-// Grid barrier with a bounded wait.  Returns false (in every thread) once any block has timed out.
+// Grid barrier with a bounded wait.  Thread 0 publishes the block's writes with a release reduction (cumulative over
+// the writes the block's threads made before __syncthreads) and polls with acquire loads.  Returns false (in every
+// thread) once any block has timed out.
 __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* err) {
     ++epoch;
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned target = epoch * gridDim.x;
-        __threadfence();
-        atomicAdd(bar, 1u);
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
         const unsigned long long t0 = global_timer_ns();
         unsigned spins = 0;
         while (ld_acquire_u32(bar) < target) {
@@ -46,38 +57,88 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& epoch, int
                 break;
             }
         }
-        __threadfence();
     }
     __syncthreads();
     return *(volatile int*)err == 0;
 }
 
-// Sum of a scene's chunk partials (component q of buffer `buf`) in a fixed tree: threads stride over the scene's chunks in
-// order, then block_sum.  Every block that needs the value computes it and obtains the same bits.
-template <int K>
+// Sum of a scene's partials (item c, component comp[q] at buf[STRIDE * c + comp[q]]) in a fixed tree: the first 256
+// threads stride over the items in order, warp butterfly, then 8 warps in order.  Every block computing it obtains the
+// same bits.  STRIDE is 3 for the tile partials and 1 for the per-chunk rhs sums.
+template <int K, int STRIDE = 3>
 __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b, int e, const int (&comp)[K],
                                            double (&tot)[K], double* red) {
 #pragma unroll
     for (int q = 0; q < K; ++q) tot[q] = 0.0;
-    for (int c = b + threadIdx.x; c < e; c += kThreads) {
+    if (threadIdx.x < kThreads) {
+        for (int c = b + threadIdx.x; c < e; c += kThreads) {
 #pragma unroll
-        for (int q = 0; q < K; ++q) tot[q] += buf[3 * c + comp[q]];
+            for (int q = 0; q < K; ++q) tot[q] += buf[STRIDE * c + comp[q]];
+        }
     }
-    block_sum<K>(tot, red);
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tot[c] += __shfl_xor_sync(0xffffffffu, tot[c], o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0 && warp < kThreads / 32) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) red[c * 32 + warp] = tot[c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < kThreads / 32; ++q) s += red[c * 32 + q];
+        tot[c] = s;
+    }
 }
 
-// Store a chunk's partials (after the block reduction) with plain stores; the next grid barrier publishes them.
+// Per-256-thread-group sum (each group reduces its own 8 warps in index order): the tile partial tree.
 template <int K>
-__device__ __forceinline__ void put_partials(double* buf, int chunk, double (&part)[K], double* red) {
-    block_sum<K>(part, red);
-    if (threadIdx.x == 0) {
+__device__ __forceinline__ void group_sum(double (&v)[K], double* red) {
 #pragma unroll
-        for (int q = 0; q < K; ++q) buf[3 * chunk + q] = part[q];
+    for (int c = 0; c < K; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g0 = (warp >> 3) << 3;
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) red[c * 32 + warp] = v[c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s += red[c * 32 + g0 + q];
+        v[c] = s;
     }
 }
 
-// Search direction at cell t for iteration k: p_k = z + beta p_{k-1} (heat.py/grid.py CG: _cg_kernel_2), or z on the
-// first iteration (p_1 = clone(z)).
+// cell m (0..3) of thread lt in a tile
+struct Cell {
+    int t, i, j, k;
+    bool ok;
+};
+
+__device__ __forceinline__ Cell tile_cell(const TileItem& ti, int n, int lt, int m) {
+    Cell c;
+    c.i = ti.i0 + m;
+    c.j = ti.j0 + (lt >> 5);
+    c.k = ti.k0 + (lt & 31);
+    c.ok = c.i < n && c.j < n && c.k < n;
+    c.t = (c.i * n + c.j) * n + c.k;
+    return c;
+}
+
+// Search direction at cell t for iteration k: p_k = z + beta p_{k-1} (warp's _cg_kernel_2), or z at k = 1.
 struct Dir {
     const float* z;
     const float* pold;
@@ -141,156 +202,210 @@ __device__ __forceinline__ float heat_diag_sum(const hf_scene& S, int i, int j, 
     return s;
 }
 
-constexpr int kLocalScenes = 32;   // scenes one block may touch (the host checks)
+// Set-up of one cell (heat.py:198-203 + k_heat_rhs/k_heat_diag; grid.py:238-248 mean removal + k_jacobi): returns
+// b, D, r for x0 (the advected T, or the previous pressure).
+template <bool HEAT>
+__device__ __forceinline__ void setup_cell(const hf_scene& S, const float* x, float mean, float hh, float c_dt,
+                                           const Cell& c, float& b, float& d, float& r) {
+    const int n = S.n;
+    const float xc = x[c.t];
+    const Vec X{x};
+    if (HEAT) {
+        b = S.hrhs[c.t];
+        if (S.cell_flags[c.t] & 1) {
+            d = 1.0f;
+            r = __fsub_rn(b, xc);
+        } else {
+            d = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(c_dt, heat_diag_sum(S, c.i, c.j, c.k))));
+            r = __fsub_rn(b, __fadd_rn(xc, __fmul_rn(c_dt, heat_nt(S, X, xc, c.t, c.i, c.j, c.k))));
+        }
+    } else {
+        b = S.rhs[c.t];
+        if (mean != 0.0f) {
+            b = __fsub_rn(b, mean);
+            S.rhs[c.t] = b;
+        }
+        const int i = c.i, j = c.j, k = c.k;
+        float sa = 0.0f;
+        if (i > 0) sa = __fadd_rn(sa, S.ax[uidx_(n, i, j, k)]);
+        if (i < n - 1) sa = __fadd_rn(sa, S.ax[uidx_(n, i + 1, j, k)]);
+        if (j > 0) sa = __fadd_rn(sa, S.ay[vidx_(n, i, j, k)]);
+        if (j < n - 1) sa = __fadd_rn(sa, S.ay[vidx_(n, i, j + 1, k)]);
+        if (k > 0) sa = __fadd_rn(sa, S.az[widx_(n, i, j, k)]);
+        if (k < n - 1) sa = __fadd_rn(sa, S.az[widx_(n, i, j, k + 1)]);
+        d = __fdiv_rn(hh, maxf_(sa, 1.0e-12f));
+        r = __fsub_rn(b, __fdiv_rn(lap_acc(S, X, xc, c.t, i, j, k), hh));
+    }
+}
 
-// Per-block copy of a scene's CG scalars.  Every block touching the scene derives them from the same partial sums,
-// so all copies agree bit for bit.
+// grid.py:140-153 k_project for the three low faces of a cell (and the high wall faces on the last layer)
+__device__ __forceinline__ void project_cell(const hf_scene& S, float* u, float* v, float* w, const float* p, float pc,
+                                             float dtr, float h, const Cell& c) {
+    const int n = S.n, nn = n * n, t = c.t, i = c.i, j = c.j, k = c.k;
+    int f = uidx_(n, i, j, k);
+    u[f] = i == 0 ? 0.0f : __fsub_rn(u[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, p[t - nn])), h));
+    f = vidx_(n, i, j, k);
+    v[f] = j == 0 ? 0.0f : __fsub_rn(v[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, p[t - n])), h));
+    f = widx_(n, i, j, k);
+    w[f] = k == 0 ? 0.0f : __fsub_rn(w[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, p[t - 1])), h));
+    if (i == n - 1) u[uidx_(n, n, j, k)] = 0.0f;
+    if (j == n - 1) v[vidx_(n, i, n, k)] = 0.0f;
+    if (k == n - 1) w[widx_(n, i, j, n)] = 0.0f;
+}
+
+// Per-block copy of a scene's CG scalars; every block derives them from the same partial sums, so all copies agree.
 struct LocalScene {
     double rz, atol_sq, bb, rr, pAp, mean;
     float alpha, beta;
     int live, iters, maxit, status;
 };
 
+__device__ __forceinline__ void init_scalars(LocalScene& L, const hf_scene& S, bool heat, const double (&tot)[3], int N) {
+    const double tol = heat ? S.heat_tol : S.cg_tol;
+    double atol = tol * sqrt(tot[0]);
+    if (atol < tol) atol = tol;
+    if (atol < 1.0e-18) atol = 1.0e-18;
+    int maxit = heat ? S.heat_maxiter : S.cg_max_iter;
+    if (maxit <= 0) maxit = N;
+    L.maxit = maxit + (maxit & 1);   // iterations run in pairs
+    L.bb = tot[0];
+    L.rr = tot[1];
+    L.rz = tot[2];
+    L.atol_sq = atol * atol;
+    L.iters = 0;
+    L.beta = 0.0f;
+    L.alpha = 0.0f;
+    L.status = isfinite(tot[1]) ? 0 : HF_SCENE_NONFINITE;
+    L.live = tot[1] > L.atol_sq && isfinite(tot[1]) && L.maxit > 0;
+}
+
+// convergence test after phase B of iteration kit (warp: kernel_2 then the residual test)
+__device__ __forceinline__ bool update_scalars(LocalScene& L, bool heat, double rr, double rz, int kit) {
+    L.iters = kit;
+    const bool above = rr > L.atol_sq;
+    L.beta = above ? __double2float_rn(rz / L.rz) : 0.0f;
+    L.rz = rz;
+    L.rr = rr;
+    if (!isfinite(rr)) L.status |= HF_SCENE_NONFINITE;
+    const bool live = above && isfinite(rr) && kit < L.maxit;
+    if (!live && above && isfinite(rr)) L.status |= heat ? HF_SCENE_HEAT_MAXITER : HF_SCENE_PRESSURE_MAXITER;
+    L.live = live;
+    return live;
+}
+
+__device__ __forceinline__ void write_stats(const hf_scene& S, const LocalScene& L, bool heat, bool timed_out, int par) {
+    hf_scene_state* st = S.state;
+    if (heat) {
+        st->status = L.status | (timed_out ? HF_SCENE_BARRIER_TIMEOUT : 0);
+        st->heat_iters = L.iters;
+        st->heat_rr = L.rr;
+        st->heat_atol = sqrt(L.atol_sq);
+        st->heat_bb = L.bb;
+        st->total_heat_iters += L.iters;
+    } else {
+        st->status |= L.status | (timed_out ? HF_SCENE_BARRIER_TIMEOUT : 0);
+        st->pressure_iters = L.iters;
+        st->pressure_rr = L.rr;
+        st->pressure_atol = sqrt(L.atol_sq);
+        st->pressure_bb = L.bb;
+        st->rhs_mean = L.mean;
+        st->total_pressure_iters += L.iters;
+        if (!timed_out) {
+            st->parity = par ^ 1;
+            st->substeps += 1;
+        }
+    }
+}
+
+// ================================================================================================== streaming
 template <bool HEAT>
-__global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
-                                                 int num_chunks, int num_scenes, double dt_d, Workspace ws) {
-    __shared__ double red[3 * (kThreads / 32)];
+__global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles,
+                                                 int num_tiles, int num_scenes, double dt_d, Workspace ws) {
+    __shared__ double red[6 * 32];
     __shared__ unsigned char s_par[kMaxScenes];
     __shared__ LocalScene loc[kLocalScenes];
     for (int s = threadIdx.x; s < num_scenes; s += kThreads) s_par[s] = (unsigned char)scenes[s].state->parity;
-    // contiguous, balanced chunk range of this block and the scenes it touches
-    const int c0 = (int)(((long long)num_chunks * blockIdx.x) / gridDim.x);
-    const int c1 = (int)(((long long)num_chunks * (blockIdx.x + 1)) / gridDim.x);
-    const int s_lo = c0 < c1 ? work[c0].scene : 0;
-    const int s_hi = c0 < c1 ? work[c1 - 1].scene : -1;
+    const int c0 = (int)(((long long)num_tiles * blockIdx.x) / gridDim.x);
+    const int c1 = (int)(((long long)num_tiles * (blockIdx.x + 1)) / gridDim.x);
+    const int s_lo = c0 < c1 ? tiles[c0].scene : 0;
+    const int s_hi = c0 < c1 ? tiles[c1 - 1].scene : -1;
     __syncthreads();
     unsigned* bar = ws.bar + (HEAT ? 0 : 1);
     unsigned* live_count = ws.live_count + (HEAT ? 0 : 1);
-    double* bufA = ws.partials;                       // phase A partials (p.Ap)
-    double* bufB = ws.partials + 3 * (size_t)num_chunks;  // prologue / phase B partials (b.b, r.r, r.z)
+    double* bufA = ws.partA;
+    double* bufB = ws.partB;
     unsigned epoch = 0;
     const float dt = (float)dt_d;
+    const int lt = threadIdx.x;
 
     // ---------------------------------------------------------------------------------------- prologue
-    // pressure: the mean of the rhs (grid.py:238-241) from the divergence kernel's chunk partials
     for (int s = s_lo; s <= s_hi; ++s) {
-        double m[1];
-        const int comp[1] = {0};
         if (!HEAT) {
-            scene_sums<1>(bufA, ws.chunk_begin[s], ws.chunk_begin[s + 1], comp, m, red);
+            double m[1];
+            const int comp[1] = {0};
+            scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[s], ws.chunk_begin[s + 1], comp, m, red);
             const int n = scenes[s].n;
             if (threadIdx.x == 0) loc[s - s_lo].mean = (double)__double2float_rn(m[0] / ((double)n * n * n));
+        } else if (threadIdx.x == 0) {
+            loc[s - s_lo].mean = 0.0;
         }
     }
     __syncthreads();
     for (int c = c0; c < c1; ++c) {
-        const WorkItem wi = work[c];
-        const hf_scene& S = scenes[wi.scene];
-        const int n = S.n, N = n * n * n, par = s_par[wi.scene];
-        const float h = (float)S.h, hh = __fmul_rn(h, h);
-        const float c_dt = __fdiv_rn(dt, hh);
-        float* x = HEAT ? S.T[par ^ 1] : S.p;
-        const Vec X{x};
+        const TileItem ti = tiles[c];
+        const hf_scene& S = scenes[ti.scene];
+        const int n = S.n, par = s_par[ti.scene];
+        const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
+        const float* x = HEAT ? S.T[par ^ 1] : S.p;
+        const float mean = (float)loc[ti.scene - s_lo].mean;
         double part[3] = {0.0, 0.0, 0.0};
-        const float mean = HEAT ? 0.0f : (float)loc[wi.scene - s_lo].mean;
-        for (int m = 0; m < kCellsPerThread; ++m) {
-            const int t = wi.first + threadIdx.x + m * kThreads;
-            if (t >= N) break;
-            int i, j, k;
-            cell_ijk(t, n, i, j, k);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const Cell cl = tile_cell(ti, n, lt, m);
+            if (!cl.ok) continue;
             float b, d, r;
-            const float xc = x[t];
-            if (HEAT) {
-                b = S.hrhs[t];
-                if (S.cell_flags[t] & 1) {
-                    d = 1.0f;
-                    r = __fsub_rn(b, xc);
-                } else {
-                    // heat.py:121-144 k_heat_diag
-                    d = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(c_dt, heat_diag_sum(S, i, j, k))));
-                    r = __fsub_rn(b, __fadd_rn(xc, __fmul_rn(c_dt, heat_nt(S, X, xc, t, i, j, k))));
-                }
-                S.hdiag[t] = d;
-            } else {
-                // grid.py:238-241 mean removal, grid.py:118-137 k_jacobi, then r = b - A x
-                b = S.rhs[t];
-                if (mean != 0.0f) {
-                    b = __fsub_rn(b, mean);
-                    S.rhs[t] = b;
-                }
-                float s = 0.0f;
-                if (i > 0) s = __fadd_rn(s, S.ax[uidx_(n, i, j, k)]);
-                if (i < n - 1) s = __fadd_rn(s, S.ax[uidx_(n, i + 1, j, k)]);
-                if (j > 0) s = __fadd_rn(s, S.ay[vidx_(n, i, j, k)]);
-                if (j < n - 1) s = __fadd_rn(s, S.ay[vidx_(n, i, j + 1, k)]);
-                if (k > 0) s = __fadd_rn(s, S.az[widx_(n, i, j, k)]);
-                if (k < n - 1) s = __fadd_rn(s, S.az[widx_(n, i, j, k + 1)]);
-                d = __fdiv_rn(hh, maxf_(s, 1.0e-12f));
-                S.pdiag[t] = d;
-                r = __fsub_rn(b, __fdiv_rn(lap_acc(S, X, xc, t, i, j, k), hh));
-            }
+            setup_cell<HEAT>(S, x, mean, hh, c_dt, cl, b, d, r);
             const float z = __fmul_rn(d, r);
-            S.cg_r[t] = r;
-            S.cg_z[t] = z;
+            (HEAT ? S.hdiag : S.pdiag)[cl.t] = d;
+            S.cg_r[cl.t] = r;
+            S.cg_z[cl.t] = z;
             part[0] += (double)b * (double)b;
             part[1] += (double)r * (double)r;
             part[2] += (double)r * (double)z;
         }
-        put_partials<3>(bufB, c, part, red);
+        group_sum<3>(part, red);
+        if (lt == 0) {
+            bufB[3 * c] = part[0];
+            bufB[3 * c + 1] = part[1];
+            bufB[3 * c + 2] = part[2];
+        }
     }
     if (!grid_barrier(bar, epoch, ws.err)) goto finish;
 
     // ------------------------------------------------------------------------------------------ iterations
     for (int kit = 1;; ++kit) {
-        // scene scalars from the previous phase B (or the prologue): convergence test, beta
         for (int s = s_lo; s <= s_hi; ++s) {
             LocalScene& L = loc[s - s_lo];
             const hf_scene& S = scenes[s];
-            const int b = ws.chunk_begin[s], e = ws.chunk_begin[s + 1];
+            const int b = ws.tile_begin[s], e = ws.tile_begin[s + 1];
             const bool owner = b >= c0 && b < c1;
             if (kit == 1) {
                 double tot[3];
                 const int comp[3] = {0, 1, 2};
                 scene_sums<3>(bufB, b, e, comp, tot, red);
                 if (threadIdx.x == 0) {
-                    const int n = S.n;
-                    const double tol = HEAT ? S.heat_tol : S.cg_tol;
-                    double atol = tol * sqrt(tot[0]);
-                    if (atol < tol) atol = tol;
-                    if (atol < 1.0e-18) atol = 1.0e-18;
-                    int maxit = HEAT ? S.heat_maxiter : S.cg_max_iter;
-                    if (maxit <= 0) maxit = n * n * n;
-                    L.maxit = maxit + (maxit & 1);   // iterations run in pairs
-                    L.bb = tot[0];
-                    L.rr = tot[1];
-                    L.rz = tot[2];
-                    L.atol_sq = atol * atol;
-                    L.iters = 0;
-                    L.beta = 0.0f;
-                    L.status = isfinite(tot[1]) ? 0 : HF_SCENE_NONFINITE;
-                    L.live = (b < e) && tot[1] > L.atol_sq && isfinite(tot[1]) && L.maxit > 0;
+                    const double mean = L.mean;
+                    init_scalars(L, S, HEAT, tot, S.n * S.n * S.n);
+                    L.mean = mean;
+                    L.live = L.live && b < e;
                     if (owner && L.live) atomicAdd(live_count, 1u);
                 }
             } else {
-                if (!loc[s - s_lo].live) continue;   // uniform: read by all threads after the last __syncthreads
+                if (!L.live) continue;   // uniform: shared value read after the last __syncthreads
                 double tot[2];
                 const int comp[2] = {1, 2};
                 scene_sums<2>(bufB, b, e, comp, tot, red);
-                if (threadIdx.x == 0) {
-                    const double rr = tot[0], rz = tot[1];
-                    L.iters = kit - 1;
-                    const bool above = rr > L.atol_sq;
-                    L.beta = above ? __double2float_rn(rz / L.rz) : 0.0f;
-                    L.rz = rz;
-                    L.rr = rr;
-                    if (!isfinite(rr)) L.status |= HF_SCENE_NONFINITE;
-                    const bool live = above && isfinite(rr) && L.iters < L.maxit;
-                    if (!live) {
-                        if (above && isfinite(rr)) L.status |= HEAT ? HF_SCENE_HEAT_MAXITER : HF_SCENE_PRESSURE_MAXITER;
-                        L.live = 0;
-                        if (owner) atomicSub(live_count, 1u);
-                    }
-                }
+                if (threadIdx.x == 0 && !update_scalars(L, HEAT, tot[0], tot[1], kit - 1) && owner) atomicSub(live_count, 1u);
             }
             __syncthreads();
             if (owner && threadIdx.x == 0 && !L.live) {
@@ -300,60 +415,55 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
                 W.atol_sq = L.atol_sq;
                 W.iters = L.iters;
                 W.status = L.status;
-                if (!HEAT) W.mean = L.mean;
+                W.mean = L.mean;
             }
             __syncthreads();
         }
         // phase A: p_k at the stencil points, Ap = A p_k, p.Ap
         for (int c = c0; c < c1; ++c) {
-            const WorkItem wi = work[c];
-            const LocalScene& L = loc[wi.scene - s_lo];
+            const TileItem ti = tiles[c];
+            const LocalScene& L = loc[ti.scene - s_lo];
             if (!L.live) continue;
-            const hf_scene& S = scenes[wi.scene];
-            const int n = S.n, N = n * n * n;
+            const hf_scene& S = scenes[ti.scene];
+            const int n = S.n;
             const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
             const Dir P{S.cg_z, S.cg_p[(kit - 1) & 1], L.beta, kit == 1};
-            float pc[kCellsPerThread], ap[kCellsPerThread];
-            // all loads of the thread's cells first, stores after: keeps every cell's loads in flight together
+            float pc[4], ap[4];
 #pragma unroll
-            for (int m = 0; m < kCellsPerThread; ++m) {
-                const int t = wi.first + threadIdx.x + m * kThreads;
-                pc[m] = 0.0f;
-                ap[m] = 0.0f;
-                if (t < N) {
-                    int i, j, k;
-                    cell_ijk(t, n, i, j, k);
-                    pc[m] = P(t);
-                    if (HEAT) {
-                        ap[m] = (__ldg(S.cell_flags + t) & 1) ? pc[m]
-                                                              : __fadd_rn(pc[m], __fmul_rn(c_dt, heat_nt(S, P, pc[m], t, i, j, k)));
-                    } else {
-                        ap[m] = __fdiv_rn(lap_acc(S, P, pc[m], t, i, j, k), hh);
-                    }
+            for (int m = 0; m < 4; ++m) {
+                const Cell cl = tile_cell(ti, n, lt, m);
+                pc[m] = ap[m] = 0.0f;
+                if (!cl.ok) continue;
+                pc[m] = P(cl.t);
+                if (HEAT) {
+                    ap[m] = (__ldg(S.cell_flags + cl.t) & 1)
+                                ? pc[m]
+                                : __fadd_rn(pc[m], __fmul_rn(c_dt, heat_nt(S, P, pc[m], cl.t, cl.i, cl.j, cl.k)));
+                } else {
+                    ap[m] = __fdiv_rn(lap_acc(S, P, pc[m], cl.t, cl.i, cl.j, cl.k), hh);
                 }
             }
             float* pnew = S.cg_p[kit & 1];
             double part[1] = {0.0};
 #pragma unroll
-            for (int m = 0; m < kCellsPerThread; ++m) {
-                const int t = wi.first + threadIdx.x + m * kThreads;
-                if (t < N) {
-                    pnew[t] = pc[m];
-                    S.cg_Ap[t] = ap[m];
-                    part[0] += (double)pc[m] * (double)ap[m];
-                }
+            for (int m = 0; m < 4; ++m) {
+                const Cell cl = tile_cell(ti, n, lt, m);
+                if (!cl.ok) continue;
+                pnew[cl.t] = pc[m];
+                S.cg_Ap[cl.t] = ap[m];
+                part[0] += (double)pc[m] * (double)ap[m];
             }
-            put_partials<1>(bufA, c, part, red);
+            group_sum<1>(part, red);
+            if (lt == 0) bufA[3 * c] = part[0];
         }
         if (!grid_barrier(bar, epoch, ws.err)) goto finish;
         if (*(volatile unsigned*)live_count == 0u) break;
-        // alpha = r.z / p.Ap of every live scene
         for (int s = s_lo; s <= s_hi; ++s) {
             LocalScene& L = loc[s - s_lo];
             if (!L.live) continue;
             double tot[1];
             const int comp[1] = {0};
-            scene_sums<1>(bufA, ws.chunk_begin[s], ws.chunk_begin[s + 1], comp, tot, red);
+            scene_sums<1>(bufA, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
             if (threadIdx.x == 0) {
                 L.pAp = tot[0];
                 L.alpha = __double2float_rn(L.rz / tot[0]);
@@ -362,338 +472,344 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
         }
         // phase B: x += alpha p, r -= alpha Ap, z = D r, r.r and r.z
         for (int c = c0; c < c1; ++c) {
-            const WorkItem wi = work[c];
-            const LocalScene& L = loc[wi.scene - s_lo];
+            const TileItem ti = tiles[c];
+            const LocalScene& L = loc[ti.scene - s_lo];
             if (!L.live) continue;
-            const hf_scene& S = scenes[wi.scene];
-            const int n = S.n, N = n * n * n, par = s_par[wi.scene];
+            const hf_scene& S = scenes[ti.scene];
+            const int n = S.n, par = s_par[ti.scene];
             float* x = HEAT ? S.T[par ^ 1] : S.p;
             const float* D = HEAT ? S.hdiag : S.pdiag;
             const float* pk = S.cg_p[kit & 1];
             const float alpha = L.alpha;
-            float xv[kCellsPerThread], rv[kCellsPerThread], zv[kCellsPerThread];
+            float xv[4], rv[4], zv[4];
 #pragma unroll
-            for (int m = 0; m < kCellsPerThread; ++m) {
-                const int t = wi.first + threadIdx.x + m * kThreads;
-                if (t < N) {
-                    xv[m] = __fadd_rn(x[t], __fmul_rn(alpha, pk[t]));
-                    rv[m] = __fsub_rn(S.cg_r[t], __fmul_rn(alpha, S.cg_Ap[t]));
-                    zv[m] = __fmul_rn(D[t], rv[m]);
-                }
+            for (int m = 0; m < 4; ++m) {
+                const Cell cl = tile_cell(ti, n, lt, m);
+                xv[m] = rv[m] = zv[m] = 0.0f;
+                if (!cl.ok) continue;
+                xv[m] = __fadd_rn(x[cl.t], __fmul_rn(alpha, pk[cl.t]));
+                rv[m] = __fsub_rn(S.cg_r[cl.t], __fmul_rn(alpha, S.cg_Ap[cl.t]));
+                zv[m] = __fmul_rn(D[cl.t], rv[m]);
             }
-            double part[3] = {0.0, 0.0, 0.0};
+            double part[2] = {0.0, 0.0};
 #pragma unroll
-            for (int m = 0; m < kCellsPerThread; ++m) {
-                const int t = wi.first + threadIdx.x + m * kThreads;
-                if (t < N) {
-                    x[t] = xv[m];
-                    S.cg_r[t] = rv[m];
-                    S.cg_z[t] = zv[m];
-                    part[1] += (double)rv[m] * (double)rv[m];
-                    part[2] += (double)rv[m] * (double)zv[m];
-                }
+            for (int m = 0; m < 4; ++m) {
+                const Cell cl = tile_cell(ti, n, lt, m);
+                if (!cl.ok) continue;
+                x[cl.t] = xv[m];
+                S.cg_r[cl.t] = rv[m];
+                S.cg_z[cl.t] = zv[m];
+                part[0] += (double)rv[m] * (double)rv[m];
+                part[1] += (double)rv[m] * (double)zv[m];
             }
-            put_partials<3>(bufB, c, part, red);
+            group_sum<2>(part, red);
+            if (lt == 0) {
+                bufB[3 * c + 1] = part[0];
+                bufB[3 * c + 2] = part[1];
+            }
         }
         if (!grid_barrier(bar, epoch, ws.err)) goto finish;
     }
-
     // -------------------------------------------------------------------- pressure epilogue: projection
     if (!HEAT) {
-        // grid.py:140-153 k_project x3 with dt/rho formed in double (grid.py:251)
         for (int c = c0; c < c1; ++c) {
-            const WorkItem wi = work[c];
-            const hf_scene& S = scenes[wi.scene];
-            const int n = S.n, N = n * n * n, nn = n * n, par = s_par[wi.scene];
+            const TileItem ti = tiles[c];
+            const hf_scene& S = scenes[ti.scene];
+            const int n = S.n, par = s_par[ti.scene];
             const float h = (float)S.h, dtr = (float)(dt_d / S.rho);
-            float *u = S.u[par ^ 1], *v = S.v[par ^ 1], *w = S.w[par ^ 1];
-            const float* p = S.p;
-            for (int m = 0; m < kCellsPerThread; ++m) {
-                const int t = wi.first + threadIdx.x + m * kThreads;
-                if (t >= N) break;
-                int i, j, k;
-                cell_ijk(t, n, i, j, k);
-                const float pc = p[t];
-                int f = uidx_(n, i, j, k);
-                u[f] = i == 0 ? 0.0f : __fsub_rn(u[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, p[t - nn])), h));
-                f = vidx_(n, i, j, k);
-                v[f] = j == 0 ? 0.0f : __fsub_rn(v[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, p[t - n])), h));
-                f = widx_(n, i, j, k);
-                w[f] = k == 0 ? 0.0f : __fsub_rn(w[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, p[t - 1])), h));
-                if (i == n - 1) u[uidx_(n, n, j, k)] = 0.0f;
-                if (j == n - 1) v[vidx_(n, i, n, k)] = 0.0f;
-                if (k == n - 1) w[widx_(n, i, j, n)] = 0.0f;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const Cell cl = tile_cell(ti, n, lt, m);
+                if (cl.ok) project_cell(S, S.u[par ^ 1], S.v[par ^ 1], S.w[par ^ 1], S.p, S.p[cl.t], dtr, h, cl);
             }
         }
     }
-
 finish:
-    // statistics (and, after the pressure solve, the end of the substep).  Owners wrote their scene records before
-    // the last barrier; every block read the parities before its first barrier, so block 0 may flip them now.
+    // Owners recorded their scene before the last barrier; every block read the parities before its first barrier,
+    // so block 0 may flip them now.
     if (blockIdx.x == 0) {
         const bool timed_out = *(volatile int*)ws.err != 0;
         for (int s = threadIdx.x; s < num_scenes; s += kThreads) {
             const hf_scene& S = scenes[s];
             if (!(S.flags & HF_FLAG_ACTIVE)) continue;
             const CgCtl& C = ws.ctl[s];
-            hf_scene_state* st = S.state;
-            if (HEAT) {
-                st->status = C.status | (timed_out ? HF_SCENE_BARRIER_TIMEOUT : 0);
-                st->heat_iters = C.iters;
-                st->heat_rr = C.rr;
-                st->heat_atol = sqrt(C.atol_sq);
-                st->heat_bb = C.bb;
-                st->total_heat_iters += C.iters;
-            } else {
-                st->status |= C.status | (timed_out ? HF_SCENE_BARRIER_TIMEOUT : 0);
-                st->pressure_iters = C.iters;
-                st->pressure_rr = C.rr;
-                st->pressure_atol = sqrt(C.atol_sq);
-                st->pressure_bb = C.bb;
-                st->rhs_mean = C.mean;
-                st->total_pressure_iters += C.iters;
-                if (!timed_out) {
-                    st->parity = s_par[s] ^ 1;
-                    st->substeps += 1;
-                }
-            }
+            LocalScene L;
+            L.bb = C.bb;
+            L.rr = C.rr;
+            L.atol_sq = C.atol_sq;
+            L.iters = C.iters;
+            L.status = C.status;
+            L.mean = C.mean;
+            write_stats(S, L, HEAT, timed_out, s_par[s]);
         }
     }
 }
 
-// ================================================================================ register-resident variant
-// Single-scene plans whose chunks fit one block per SM keep the whole CG state of their cells in registers: every
-// thread owns the same cells for the entire solve (x, r, z, p, D and Ap never leave the SM); per iteration only the
-// search direction p (phase A) and z (phase B) are published to global memory, because neighbouring blocks read them
-// at their stencil points.  The chunk -> (group, thread) mapping and the reduction tree are those of k_pcg (256
-// virtual threads x 4 cells per chunk, warp butterfly, 8 warps in order), so both kernels produce the same bits.
-//
-// Block = `groups` x 256 threads; group g owns chunks c0 + g + groups*q (q < MAXC) of the block's contiguous range.
-template <int K>
-__device__ __forceinline__ void group_sum(double (&v)[K], double* red) {
-    // red: K * (blockDim.x / 32) doubles; every 256-thread group reduces its own 8 warps in index order
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int g0 = (warp >> 3) << 3;   // first warp of this group
-    __syncthreads();
-    if (lane == 0) {
-#pragma unroll
-        for (int c = 0; c < K; ++c) red[c * nw + warp] = v[c];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-        double s = 0.0;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) s += red[c * nw + g0 + q];
-        v[c] = s;
+// ============================================================================================ TMA staging
+// Box geometry of the tiled pressure stencil (elements, innermost k first), all at 16-byte aligned k origins:
+//   z / p_old : k in [k0-4, k0+36), j in [j0-1, j0+9), i in [i0-1, i0+5)   (one-cell halo; k widened to alignment)
+//   alpha_f x : k in [k0, k0+32),   j in [j0, j0+8),   i in [i0, i0+5)     (low faces of the tile + next i layer)
+//   alpha_f y : k in [k0, k0+32),   j in [j0, j0+9),   i in [i0, i0+4)
+//   alpha_f z : k in [k0, k0+36),   j in [j0, j0+8),   i in [i0, i0+4)
+// Out-of-range elements are zero-filled by the copy engine and never used (domain faces are skipped).
+constexpr int kBZ = 40 * 10 * 6, kBX = 32 * 8 * 5, kBY = 32 * 9 * 4, kBW = 36 * 8 * 4;
+constexpr int kSlotFloats = 2 * kBZ + kBX + kBY + kBW;   // 8384 floats = 33,536 bytes (a multiple of 128)
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// bounded wait for the given phase; returns false on timeout
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phase) {
+    const unsigned long long t0 = global_timer_ns();
+    for (unsigned spins = 0;; ++spins) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(smem_addr(bar)), "r"(phase)
+            : "memory");
+        if (ok) return true;
+        if ((spins & 63u) == 63u && global_timer_ns() - t0 > kBarrierTimeoutNs) return false;
     }
 }
 
-// scene_sums for blocks of any size: the first 256 threads form the same tree as scene_sums in a 256-thread block.
-template <int K>
-__device__ __forceinline__ void scene_sums_g(const double* __restrict__ buf, int b, int e, const int (&comp)[K],
-                                             double (&tot)[K], double* red) {
-#pragma unroll
-    for (int q = 0; q < K; ++q) tot[q] = 0.0;
-    if (threadIdx.x < kThreads) {
-        for (int c = b + threadIdx.x; c < e; c += kThreads) {
-#pragma unroll
-            for (int q = 0; q < K; ++q) tot[q] += buf[3 * c + comp[q]];
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) tot[c] += __shfl_xor_sync(0xffffffffu, tot[c], o);
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0 && warp < kThreads / 32) {
-#pragma unroll
-        for (int c = 0; c < K; ++c) red[c * (kThreads / 32) + warp] = tot[c];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-        double sum = 0.0;
-#pragma unroll
-        for (int q = 0; q < kThreads / 32; ++q) sum += red[c * (kThreads / 32) + q];
-        tot[c] = sum;
-    }
+__device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int x, int y, int z, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
 }
 
-template <bool HEAT, int MAXC>
-__global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1) k_pcg_res(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
-                                                    int num_chunks, int num_scenes, double dt_d, Workspace ws) {
-    constexpr int CPT = kCellsPerThread * MAXC;   // cells per thread
-    __shared__ double red[3 * 32];
+// ======================================================================================= register-resident
+// Block = `groups` x 256 threads; group g owns tiles c0 + g + groups*q (q < MAXC) of the block's contiguous range.
+template <bool HEAT, int MAXC, bool TMA>
+__global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
+    k_pcg_res(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int num_tiles, int num_scenes,
+              double dt_d, Workspace ws, const __grid_constant__ TileMaps maps) {
+    constexpr int CPT = 4 * MAXC;   // cells per thread
+    extern __shared__ __align__(128) float sm_raw[];
+    // TMA destinations must be 128-byte aligned: the launch adds 128 bytes of slack
+    float* sm_boxes = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
+    __shared__ double red[6 * 32];
     __shared__ LocalScene Ls;
+    __shared__ __align__(8) unsigned long long mbar[4 * 3];
     const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
-    const int c0 = (int)(((long long)num_chunks * blockIdx.x) / gridDim.x);
-    const int c1 = (int)(((long long)num_chunks * (blockIdx.x + 1)) / gridDim.x);
-    const int sidx = work[c0].scene;                       // one scene per plan on this path
+    const int c0 = (int)(((long long)num_tiles * blockIdx.x) / gridDim.x);
+    const int c1 = (int)(((long long)num_tiles * (blockIdx.x + 1)) / gridDim.x);
+    const int sidx = tiles[c0].scene;   // one scene per plan on this path
     const hf_scene& S = scenes[sidx];
-    const int n = S.n, N = n * n * n, nn = n * n;
+    const int n = S.n, N = n * n * n;
     const int par = S.state->parity;
     unsigned* bar = ws.bar + (HEAT ? 0 : 1);
     unsigned epoch = 0;
     const float dt = (float)dt_d;
     const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
-    double* bufA = ws.partials;
-    double* bufB = ws.partials + 3 * (size_t)num_chunks;
-    const int cb = ws.chunk_begin[sidx], ce = ws.chunk_begin[sidx + 1];
+    double* bufA = ws.partA;
+    double* bufB = ws.partB;
+    const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
     float* xg = HEAT ? S.T[par ^ 1] : S.p;
     float* zg = S.cg_z;
+    TileItem my[MAXC];
+    bool have[MAXC];
+#pragma unroll
+    for (int q = 0; q < MAXC; ++q) {
+        const int c = c0 + g + groups * q;
+        have[q] = c < c1;
+        my[q] = tiles[have[q] ? c : c0];
+    }
+    unsigned phase_bit = 0;
+    if (TMA && lt == 0) {
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) mbar_init(&mbar[g * MAXC + q], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
 
-    // cells of this thread: chunk q, sub-cell m -> slot q*4+m (chunks of a one-scene plan are consecutive)
     float x[CPT], r[CPT], z[CPT], p[CPT], D[CPT], Ap[CPT];
-    const int cell0 = (c0 + g - cb) * kChunk + lt;
-    const int cstep = groups * kChunk;
-    const int clim = min(N, (c1 - cb) * kChunk);
-#define TCELL(s_) (cell0 + ((s_) / kCellsPerThread) * cstep + ((s_) % kCellsPerThread) * kThreads)
-#define TVALID(t_) ((t_) < clim)
-    // ------------------------------------------------------------------ prologue (as k_pcg, values kept in regs)
+    // ------------------------------------------------------------------ prologue (values kept in registers)
     float mean = 0.0f;
     if (!HEAT) {
         double mm[1];
         const int comp[1] = {0};
-        scene_sums_g<1>(bufA, cb, ce, comp, mm, red);   
+        scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red);
         mean = __double2float_rn(mm[0] / ((double)n * n * n));
-    }
-    {
-        const Vec X{xg};
-#pragma unroll
-        for (int s = 0; s < CPT; ++s) {
-            x[s] = r[s] = z[s] = p[s] = D[s] = Ap[s] = 0.0f;
-            const int t = TCELL(s);
-            if (!TVALID(t)) continue;
-            int i, j, k;
-            cell_ijk(t, n, i, j, k);
-            float b, d, rr;
-            const float xc = xg[t];
-            if (HEAT) {
-                b = S.hrhs[t];
-                if (S.cell_flags[t] & 1) {
-                    d = 1.0f;
-                    rr = __fsub_rn(b, xc);
-                } else {
-                    d = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(c_dt, heat_diag_sum(S, i, j, k))));
-                    rr = __fsub_rn(b, __fadd_rn(xc, __fmul_rn(c_dt, heat_nt(S, X, xc, t, i, j, k))));
-                }
-            } else {
-                b = S.rhs[t];
-                if (mean != 0.0f) {
-                    b = __fsub_rn(b, mean);
-                    S.rhs[t] = b;
-                }
-                float sa = 0.0f;
-                if (i > 0) sa = __fadd_rn(sa, S.ax[uidx_(n, i, j, k)]);
-                if (i < n - 1) sa = __fadd_rn(sa, S.ax[uidx_(n, i + 1, j, k)]);
-                if (j > 0) sa = __fadd_rn(sa, S.ay[vidx_(n, i, j, k)]);
-                if (j < n - 1) sa = __fadd_rn(sa, S.ay[vidx_(n, i, j + 1, k)]);
-                if (k > 0) sa = __fadd_rn(sa, S.az[widx_(n, i, j, k)]);
-                if (k < n - 1) sa = __fadd_rn(sa, S.az[widx_(n, i, j, k + 1)]);
-                d = __fdiv_rn(hh, maxf_(sa, 1.0e-12f));
-                rr = __fsub_rn(b, __fdiv_rn(lap_acc(S, X, xc, t, i, j, k), hh));
-            }
-            x[s] = xc;
-            D[s] = d;
-            r[s] = rr;
-            z[s] = __fmul_rn(d, rr);
-            Ap[s] = b;   // holds b until the partial sums below
-        }
     }
 #pragma unroll
     for (int q = 0; q < MAXC; ++q) {
         double part[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int m = 0; m < kCellsPerThread; ++m) {
-            const int s = q * kCellsPerThread + m, t = TCELL(s);
-            if (!TVALID(t)) continue;
-            zg[t] = z[s];
-            part[0] += (double)Ap[s] * (double)Ap[s];
-            part[1] += (double)r[s] * (double)r[s];
-            part[2] += (double)r[s] * (double)z[s];
+        for (int m = 0; m < 4; ++m) {
+            const int s = q * 4 + m;
+            x[s] = r[s] = z[s] = p[s] = D[s] = Ap[s] = 0.0f;
+            const Cell cl = tile_cell(my[q], n, lt, m);
+            if (!have[q] || !cl.ok) continue;
+            float b, d, rr;
+            setup_cell<HEAT>(S, xg, mean, hh, c_dt, cl, b, d, rr);
+            x[s] = xg[cl.t];
+            D[s] = d;
+            r[s] = rr;
+            z[s] = __fmul_rn(d, rr);
+            zg[cl.t] = z[s];
+            part[0] += (double)b * (double)b;
+            part[1] += (double)rr * (double)rr;
+            part[2] += (double)rr * (double)z[s];
         }
         group_sum<3>(part, red);
         const int c = c0 + g + groups * q;
-        if (lt == 0 && c < c1) {
+        if (lt == 0 && have[q]) {
             bufB[3 * c] = part[0];
             bufB[3 * c + 1] = part[1];
             bufB[3 * c + 2] = part[2];
         }
     }
+    // the face fractions of the tiles stay in shared memory for the whole solve
+    if (TMA && lt == 0) {
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            if (!have[q]) continue;
+            float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+            unsigned long long* mb = &mbar[g * MAXC + q];
+            mbar_expect_tx(mb, (unsigned)((kBX + kBY + kBW) * sizeof(float)));
+            tma_load_3d(slot + 2 * kBZ, &maps.ax, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + 2 * kBZ + kBX, &maps.ayc, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + 2 * kBZ + kBX + kBY, &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
+        }
+    }
+    if (TMA) {
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], phase_bit) && ok;
+        if (!ok) atomicExch(ws.err, 1);
+        phase_bit ^= 1u;
+    }
     if (!grid_barrier(bar, epoch, ws.err)) goto finish;
     {
         double tot[3];
         const int comp[3] = {0, 1, 2};
-        scene_sums_g<3>(bufB, cb, ce, comp, tot, red);
+        scene_sums<3>(bufB, cb, ce, comp, tot, red);
         if (threadIdx.x == 0) {
-            const double tol = HEAT ? S.heat_tol : S.cg_tol;
-            double atol = tol * sqrt(tot[0]);
-            if (atol < tol) atol = tol;
-            if (atol < 1.0e-18) atol = 1.0e-18;
-            int maxit = HEAT ? S.heat_maxiter : S.cg_max_iter;
-            if (maxit <= 0) maxit = N;
-            Ls.maxit = maxit + (maxit & 1);
-            Ls.bb = tot[0];
-            Ls.rr = tot[1];
-            Ls.rz = tot[2];
-            Ls.atol_sq = atol * atol;
-            Ls.iters = 0;
-            Ls.beta = 0.0f;
+            init_scalars(Ls, S, HEAT, tot, N);
             Ls.mean = (double)mean;
-            Ls.status = isfinite(tot[1]) ? 0 : HF_SCENE_NONFINITE;
-            Ls.live = tot[1] > Ls.atol_sq && isfinite(tot[1]) && Ls.maxit > 0;
         }
         __syncthreads();
     }
     // ------------------------------------------------------------------------------------------ iterations
     for (int kit = 1; Ls.live; ++kit) {
-        // phase A: p_k (own cells from registers, neighbours from z and p_{k-1} in global memory), Ap, p.Ap
+        // phase A: p_k, Ap = A p_k, p.Ap
         const float beta = Ls.beta;
         const bool first = kit == 1;
         const float* pold = S.cg_p[(kit - 1) & 1];
         float* pnew = S.cg_p[kit & 1];
-        const Dir P{zg, pold, beta, first};
+        if (TMA) {
+            // stage z and p_{k-1} (with halo) of every tile of the group, then form p_k in place over the z box
+            if (lt == 0) {
+                asm volatile("fence.proxy.async.global;" ::: "memory");
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 #pragma unroll
-        for (int s = 0; s < CPT; ++s) {
-            const int t = TCELL(s);
-            if (!TVALID(t)) continue;
-            const float pc = first ? z[s] : __fadd_rn(z[s], __fmul_rn(beta, p[s]));
-            int i, j, k;
-            cell_ijk(t, n, i, j, k);
-            if (HEAT) {
-                Ap[s] = (__ldg(S.cell_flags + t) & 1) ? pc : __fadd_rn(pc, __fmul_rn(c_dt, heat_nt(S, P, pc, t, i, j, k)));
-            } else {
-                Ap[s] = __fdiv_rn(lap_acc(S, P, pc, t, i, j, k), hh);
+                for (int q = 0; q < MAXC; ++q) {
+                    if (!have[q]) continue;
+                    float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                    unsigned long long* mb = &mbar[g * MAXC + q];
+                    mbar_expect_tx(mb, (unsigned)((first ? 1 : 2) * kBZ * sizeof(float)));
+                    tma_load_3d(slot, &maps.z, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
+                    if (!first)
+                        tma_load_3d(slot + kBZ, ((kit - 1) & 1) ? &maps.p1 : &maps.p0, my[q].k0 - 4, my[q].j0 - 1,
+                                    my[q].i0 - 1, mb);
+                }
             }
-            p[s] = pc;
+            bool ok = true;
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q)
+                if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], phase_bit) && ok;
+            if (!ok) atomicExch(ws.err, 1);
+            phase_bit ^= 1u;
+            if (!first) {
+#pragma unroll
+                for (int q = 0; q < MAXC; ++q) {
+                    if (!have[q]) continue;
+                    float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                    for (int e = lt; e < kBZ; e += 256) slot[e] = __fadd_rn(slot[e], __fmul_rn(beta, slot[kBZ + e]));
+                }
+            }
+            asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory");
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                const float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                const float* Pb = slot;
+                const float* axb = slot + 2 * kBZ;
+                const float* ayb = axb + kBX;
+                const float* azb = ayb + kBY;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int s = q * 4 + m;
+                    const Cell cl = tile_cell(my[q], n, lt, m);
+                    if (!have[q] || !cl.ok) continue;
+                    const float pc = first ? z[s] : __fadd_rn(z[s], __fmul_rn(beta, p[s]));
+                    const int bi = cl.i - my[q].i0, bj = cl.j - my[q].j0, bk = cl.k - my[q].k0;
+                    const int o = (bi + 1) * 400 + (bj + 1) * 40 + (bk + 4);
+                    float acc = 0.0f;
+                    if (cl.i > 0) acc = __fadd_rn(acc, __fmul_rn(axb[bi * 256 + bj * 32 + bk], __fsub_rn(pc, Pb[o - 400])));
+                    if (cl.i < n - 1)
+                        acc = __fadd_rn(acc, __fmul_rn(axb[(bi + 1) * 256 + bj * 32 + bk], __fsub_rn(pc, Pb[o + 400])));
+                    if (cl.j > 0) acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + bj * 32 + bk], __fsub_rn(pc, Pb[o - 40])));
+                    if (cl.j < n - 1)
+                        acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + (bj + 1) * 32 + bk], __fsub_rn(pc, Pb[o + 40])));
+                    if (cl.k > 0) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk], __fsub_rn(pc, Pb[o - 1])));
+                    if (cl.k < n - 1)
+                        acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk + 1], __fsub_rn(pc, Pb[o + 1])));
+                    Ap[s] = __fdiv_rn(acc, hh);
+                    p[s] = pc;
+                }
+            }
+        } else {
+            const Dir P{zg, pold, beta, first};
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int s = q * 4 + m;
+                    const Cell cl = tile_cell(my[q], n, lt, m);
+                    if (!have[q] || !cl.ok) continue;
+                    const float pc = first ? z[s] : __fadd_rn(z[s], __fmul_rn(beta, p[s]));
+                    if (HEAT) {
+                        Ap[s] = (__ldg(S.cell_flags + cl.t) & 1)
+                                    ? pc
+                                    : __fadd_rn(pc, __fmul_rn(c_dt, heat_nt(S, P, pc, cl.t, cl.i, cl.j, cl.k)));
+                    } else {
+                        Ap[s] = __fdiv_rn(lap_acc(S, P, pc, cl.t, cl.i, cl.j, cl.k), hh);
+                    }
+                    p[s] = pc;
+                }
+            }
         }
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) {
             double part[1] = {0.0};
 #pragma unroll
-            for (int m = 0; m < kCellsPerThread; ++m) {
-                const int s = q * kCellsPerThread + m, t = TCELL(s);
-                if (!TVALID(t)) continue;
-                pnew[t] = p[s];
+            for (int m = 0; m < 4; ++m) {
+                const int s = q * 4 + m;
+                const Cell cl = tile_cell(my[q], n, lt, m);
+                if (!have[q] || !cl.ok) continue;
+                pnew[cl.t] = p[s];
                 part[0] += (double)p[s] * (double)Ap[s];
             }
             group_sum<1>(part, red);
             const int c = c0 + g + groups * q;
-            if (lt == 0 && c < c1) bufA[3 * c] = part[0];
+            if (lt == 0 && have[q]) bufA[3 * c] = part[0];
         }
         if (!grid_barrier(bar, epoch, ws.err)) goto finish;
         {
             double tot[1];
             const int comp[1] = {0};
-            scene_sums_g<1>(bufA, cb, ce, comp, tot, red);
+            scene_sums<1>(bufA, cb, ce, comp, tot, red);
             if (threadIdx.x == 0) {
                 Ls.pAp = tot[0];
                 Ls.alpha = __double2float_rn(Ls.rz / tot[0]);
@@ -706,19 +822,20 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         for (int q = 0; q < MAXC; ++q) {
             double part[2] = {0.0, 0.0};
 #pragma unroll
-            for (int m = 0; m < kCellsPerThread; ++m) {
-                const int s = q * kCellsPerThread + m, t = TCELL(s);
-                if (!TVALID(t)) continue;
+            for (int m = 0; m < 4; ++m) {
+                const int s = q * 4 + m;
+                const Cell cl = tile_cell(my[q], n, lt, m);
+                if (!have[q] || !cl.ok) continue;
                 x[s] = __fadd_rn(x[s], __fmul_rn(alpha, p[s]));
                 r[s] = __fsub_rn(r[s], __fmul_rn(alpha, Ap[s]));
                 z[s] = __fmul_rn(D[s], r[s]);
-                zg[t] = z[s];
+                zg[cl.t] = z[s];
                 part[0] += (double)r[s] * (double)r[s];
                 part[1] += (double)r[s] * (double)z[s];
             }
             group_sum<2>(part, red);
             const int c = c0 + g + groups * q;
-            if (lt == 0 && c < c1) {
+            if (lt == 0 && have[q]) {
                 bufB[3 * c + 1] = part[0];
                 bufB[3 * c + 2] = part[1];
             }
@@ -727,91 +844,347 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         {
             double tot[2];
             const int comp[2] = {1, 2};
-            scene_sums_g<2>(bufB, cb, ce, comp, tot, red);
-            if (threadIdx.x == 0) {
-                const double rr = tot[0], rz = tot[1];
-                Ls.iters = kit;
-                const bool above = rr > Ls.atol_sq;
-                Ls.beta = above ? __double2float_rn(rz / Ls.rz) : 0.0f;
-                Ls.rz = rz;
-                Ls.rr = rr;
-                if (!isfinite(rr)) Ls.status |= HF_SCENE_NONFINITE;
-                const bool live = above && isfinite(rr) && kit < Ls.maxit;
-                if (!live && above && isfinite(rr)) Ls.status |= HEAT ? HF_SCENE_HEAT_MAXITER : HF_SCENE_PRESSURE_MAXITER;
-                Ls.live = live;
-            }
+            scene_sums<2>(bufB, cb, ce, comp, tot, red);
+            if (threadIdx.x == 0) update_scalars(Ls, HEAT, tot[0], tot[1], kit);
             __syncthreads();
         }
     }
     // ------------------------------------------------------------------ write the solution back
 #pragma unroll
-    for (int s = 0; s < CPT; ++s)
-        if (TVALID(TCELL(s))) xg[TCELL(s)] = x[s];
+    for (int q = 0; q < MAXC; ++q) {
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const Cell cl = tile_cell(my[q], n, lt, m);
+            if (have[q] && cl.ok) xg[cl.t] = x[q * 4 + m];
+        }
+    }
     if (!HEAT) {
         // grid.py:140-153: the projection reads p at neighbour cells owned by other blocks
         if (!grid_barrier(bar, epoch, ws.err)) goto finish;
         const float dtr = (float)(dt_d / S.rho);
-        float *u = S.u[par ^ 1], *v = S.v[par ^ 1], *w = S.w[par ^ 1];
-        const float* pp = S.p;
 #pragma unroll
-        for (int s = 0; s < CPT; ++s) {
-            const int t = TCELL(s);
-            if (!TVALID(t)) continue;
-            int i, j, k;
-            cell_ijk(t, n, i, j, k);
-            const float pc = x[s];
-            int f = uidx_(n, i, j, k);
-            u[f] = i == 0 ? 0.0f : __fsub_rn(u[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, pp[t - nn])), h));
-            f = vidx_(n, i, j, k);
-            v[f] = j == 0 ? 0.0f : __fsub_rn(v[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, pp[t - n])), h));
-            f = widx_(n, i, j, k);
-            w[f] = k == 0 ? 0.0f : __fsub_rn(w[f], __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, pp[t - 1])), h));
-            if (i == n - 1) u[uidx_(n, n, j, k)] = 0.0f;
-            if (j == n - 1) v[vidx_(n, i, n, k)] = 0.0f;
-            if (k == n - 1) w[widx_(n, i, j, n)] = 0.0f;
-        }
-    }
-finish:
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const bool timed_out = *(volatile int*)ws.err != 0;
-        hf_scene_state* st = S.state;
-        if (HEAT) {
-            st->status = Ls.status | (timed_out ? HF_SCENE_BARRIER_TIMEOUT : 0);
-            st->heat_iters = Ls.iters;
-            st->heat_rr = Ls.rr;
-            st->heat_atol = sqrt(Ls.atol_sq);
-            st->heat_bb = Ls.bb;
-            st->total_heat_iters += Ls.iters;
-        } else {
-            st->status |= Ls.status | (timed_out ? HF_SCENE_BARRIER_TIMEOUT : 0);
-            st->pressure_iters = Ls.iters;
-            st->pressure_rr = Ls.rr;
-            st->pressure_atol = sqrt(Ls.atol_sq);
-            st->pressure_bb = Ls.bb;
-            st->rhs_mean = Ls.mean;
-            st->total_pressure_iters += Ls.iters;
-            if (!timed_out) {
-                st->parity = par ^ 1;
-                st->substeps += 1;
+        for (int q = 0; q < MAXC; ++q) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const Cell cl = tile_cell(my[q], n, lt, m);
+                if (have[q] && cl.ok)
+                    project_cell(S, S.u[par ^ 1], S.v[par ^ 1], S.w[par ^ 1], S.p, x[q * 4 + m], dtr, h, cl);
             }
         }
     }
+finish:
+    if (TMA && *(volatile int*)ws.err) {
+        // leave no copy in flight: a timed-out wait is retried (bounded) before the block exits
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) mbar_wait(&mbar[g * MAXC + q], phase_bit ^ 1u);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, HEAT, *(volatile int*)ws.err != 0, par);
 }
 
-#undef TCELL
-#undef TVALID
-
-const void* pcg_resident_kernel(bool heat, int maxc) {
-    if (heat) {
-        if (maxc == 1) return (const void*)k_pcg_res<true, 1>;
-        if (maxc == 2) return (const void*)k_pcg_res<true, 2>;
-        return (const void*)k_pcg_res<true, 3>;
+// ============================================================================= resident pressure CG with TMA staging
+// Same mapping, arithmetic and reduction trees as k_pcg / k_pcg_res, with less state per thread: the search direction
+// of the own cells is read from the staged box (its centre), A p is parked in the p_{k-1} box (dead once p_k is
+// formed), so a thread keeps only x, r and D of its cells in registers.  One group reduction per phase covers all the
+// thread's tiles.
+template <int MAXC>
+__global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
+    k_pcg_tma(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int num_tiles, int num_scenes,
+              double dt_d, Workspace ws, const __grid_constant__ TileMaps maps) {
+    constexpr int CPT = 4 * MAXC;
+    extern __shared__ __align__(128) float sm_raw[];
+    float* sm_boxes = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
+    __shared__ double red[6 * 32];
+    __shared__ LocalScene Ls;
+    __shared__ __align__(8) unsigned long long mbar[4 * 3];
+    const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
+    const int c0 = (int)(((long long)num_tiles * blockIdx.x) / gridDim.x);
+    const int c1 = (int)(((long long)num_tiles * (blockIdx.x + 1)) / gridDim.x);
+    const int sidx = tiles[c0].scene;
+    const hf_scene& S = scenes[sidx];
+    const int n = S.n, N = n * n * n;
+    const int par = S.state->parity;
+    unsigned* bar = ws.bar + 1;
+    unsigned epoch = 0;
+    const float h = (float)S.h, hh = __fmul_rn(h, h);
+    double* bufA = ws.partA;
+    double* bufB = ws.partB;
+    const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
+    float* xg = S.p;
+    float* zg = S.cg_z;
+    TileItem my[MAXC];
+    bool have[MAXC];
+#pragma unroll
+    for (int q = 0; q < MAXC; ++q) {
+        const int c = c0 + g + groups * q;
+        have[q] = c < c1;
+        my[q] = tiles[have[q] ? c : c0];
     }
-    if (maxc == 1) return (const void*)k_pcg_res<false, 1>;
-    if (maxc == 2) return (const void*)k_pcg_res<false, 2>;
-    return (const void*)k_pcg_res<false, 3>;
+    unsigned phase_bit = 0;
+    if (lt == 0) {
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) mbar_init(&mbar[g * MAXC + q], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    float x[CPT], r[CPT], D[CPT];
+    // ------------------------------------------------------------------------------------------ prologue
+    float mean;
+    {
+        double mm[1];
+        const int comp[1] = {0};
+        scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red);
+        mean = __double2float_rn(mm[0] / ((double)n * n * n));
+    }
+    {
+        double part[3 * MAXC];
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            part[3 * q] = part[3 * q + 1] = part[3 * q + 2] = 0.0;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int s = q * 4 + m;
+                x[s] = r[s] = D[s] = 0.0f;
+                const Cell cl = tile_cell(my[q], n, lt, m);
+                if (!have[q] || !cl.ok) continue;
+                float b, d, rr;
+                setup_cell<false>(S, xg, mean, hh, 0.0f, cl, b, d, rr);
+                const float z = __fmul_rn(d, rr);
+                x[s] = xg[cl.t];
+                D[s] = d;
+                r[s] = rr;
+                zg[cl.t] = z;
+                part[3 * q] += (double)b * (double)b;
+                part[3 * q + 1] += (double)rr * (double)rr;
+                part[3 * q + 2] += (double)rr * (double)z;
+            }
+        }
+        group_sum<3 * MAXC>(part, red);
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            const int c = c0 + g + groups * q;
+            if (lt == 0 && have[q]) {
+                bufB[3 * c] = part[3 * q];
+                bufB[3 * c + 1] = part[3 * q + 1];
+                bufB[3 * c + 2] = part[3 * q + 2];
+            }
+        }
+    }
+    // the face fractions of the tiles stay in shared memory for the whole solve
+    if (lt == 0) {
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            if (!have[q]) continue;
+            float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+            unsigned long long* mb = &mbar[g * MAXC + q];
+            mbar_expect_tx(mb, (unsigned)((kBX + kBY + kBW) * sizeof(float)));
+            tma_load_3d(slot + 2 * kBZ, &maps.ax, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + 2 * kBZ + kBX, &maps.ayc, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + 2 * kBZ + kBX + kBY, &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
+        }
+    }
+    {
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], phase_bit) && ok;
+        if (!ok) atomicExch(ws.err, 1);
+        phase_bit ^= 1u;
+    }
+    if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+    {
+        double tot[3];
+        const int comp[3] = {0, 1, 2};
+        scene_sums<3>(bufB, cb, ce, comp, tot, red);
+        if (threadIdx.x == 0) {
+            init_scalars(Ls, S, false, tot, N);
+            Ls.mean = (double)mean;
+        }
+        __syncthreads();
+    }
+    // ------------------------------------------------------------------------------------------ iterations
+    for (int kit = 1; Ls.live; ++kit) {
+        const float beta = Ls.beta;
+        const bool first = kit == 1;
+        float* pnew = S.cg_p[kit & 1];
+        // phase A: stage z and p_{k-1} with halo, form p_k in place, Ap from shared memory
+        if (lt == 0) {
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                if (!have[q]) continue;
+                float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                unsigned long long* mb = &mbar[g * MAXC + q];
+                mbar_expect_tx(mb, (unsigned)((first ? 1 : 2) * kBZ * sizeof(float)));
+                tma_load_3d(slot, &maps.z, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
+                if (!first)
+                    tma_load_3d(slot + kBZ, ((kit - 1) & 1) ? &maps.p1 : &maps.p0, my[q].k0 - 4, my[q].j0 - 1,
+                                my[q].i0 - 1, mb);
+            }
+        }
+        {
+            bool ok = true;
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q)
+                if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], phase_bit) && ok;
+            if (!ok) atomicExch(ws.err, 1);
+            phase_bit ^= 1u;
+        }
+        if (!first) {
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                if (!have[q]) continue;
+                float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                for (int e = lt; e < kBZ; e += 256) slot[e] = __fadd_rn(slot[e], __fmul_rn(beta, slot[kBZ + e]));
+            }
+        }
+        asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory");
+        {
+            double part[MAXC];
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                part[q] = 0.0;
+                float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                const float* Pb = slot;
+                float* Apb = slot + kBZ;   // the p_{k-1} box is dead now: A p goes to its centre
+                const float* axb = slot + 2 * kBZ;
+                const float* ayb = axb + kBX;
+                const float* azb = ayb + kBY;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const Cell cl = tile_cell(my[q], n, lt, m);
+                    if (!have[q] || !cl.ok) continue;
+                    const int bi = m, bj = lt >> 5, bk = lt & 31;
+                    const int o = (bi + 1) * 400 + (bj + 1) * 40 + (bk + 4);
+                    const float pc = Pb[o];
+                    float acc = 0.0f;
+                    if (cl.i > 0) acc = __fadd_rn(acc, __fmul_rn(axb[bi * 256 + bj * 32 + bk], __fsub_rn(pc, Pb[o - 400])));
+                    if (cl.i < n - 1)
+                        acc = __fadd_rn(acc, __fmul_rn(axb[(bi + 1) * 256 + bj * 32 + bk], __fsub_rn(pc, Pb[o + 400])));
+                    if (cl.j > 0) acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + bj * 32 + bk], __fsub_rn(pc, Pb[o - 40])));
+                    if (cl.j < n - 1)
+                        acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + (bj + 1) * 32 + bk], __fsub_rn(pc, Pb[o + 40])));
+                    if (cl.k > 0) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk], __fsub_rn(pc, Pb[o - 1])));
+                    if (cl.k < n - 1)
+                        acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk + 1], __fsub_rn(pc, Pb[o + 1])));
+                    const float ap = __fdiv_rn(acc, hh);
+                    Apb[o] = ap;
+                    pnew[cl.t] = pc;
+                    part[q] += (double)pc * (double)ap;
+                }
+            }
+            group_sum<MAXC>(part, red);
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                const int c = c0 + g + groups * q;
+                if (lt == 0 && have[q]) bufA[3 * c] = part[q];
+            }
+        }
+        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        {
+            double tot[1];
+            const int comp[1] = {0};
+            scene_sums<1>(bufA, cb, ce, comp, tot, red);
+            if (threadIdx.x == 0) {
+                Ls.pAp = tot[0];
+                Ls.alpha = __double2float_rn(Ls.rz / tot[0]);
+            }
+            __syncthreads();
+        }
+        // phase B: x += alpha p, r -= alpha Ap, z = D r; publish z; r.r and r.z
+        {
+            const float alpha = Ls.alpha;
+            double part[2 * MAXC];
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                part[2 * q] = part[2 * q + 1] = 0.0;
+                const float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int s = q * 4 + m;
+                    const Cell cl = tile_cell(my[q], n, lt, m);
+                    if (!have[q] || !cl.ok) continue;
+                    const int o = (m + 1) * 400 + ((lt >> 5) + 1) * 40 + ((lt & 31) + 4);
+                    x[s] = __fadd_rn(x[s], __fmul_rn(alpha, slot[o]));
+                    r[s] = __fsub_rn(r[s], __fmul_rn(alpha, slot[kBZ + o]));
+                    const float z = __fmul_rn(D[s], r[s]);
+                    zg[cl.t] = z;
+                    part[2 * q] += (double)r[s] * (double)r[s];
+                    part[2 * q + 1] += (double)r[s] * (double)z;
+                }
+            }
+            group_sum<2 * MAXC>(part, red);
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                const int c = c0 + g + groups * q;
+                if (lt == 0 && have[q]) {
+                    bufB[3 * c + 1] = part[2 * q];
+                    bufB[3 * c + 2] = part[2 * q + 1];
+                }
+            }
+        }
+        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        {
+            double tot[2];
+            const int comp[2] = {1, 2};
+            scene_sums<2>(bufB, cb, ce, comp, tot, red);
+            if (threadIdx.x == 0) update_scalars(Ls, false, tot[0], tot[1], kit);
+            __syncthreads();
+        }
+    }
+    // ------------------------------------------------------------------ write p back, then project the faces
+#pragma unroll
+    for (int q = 0; q < MAXC; ++q) {
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const Cell cl = tile_cell(my[q], n, lt, m);
+            if (have[q] && cl.ok) xg[cl.t] = x[q * 4 + m];
+        }
+    }
+    if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+    {
+        const float dtr = (float)(dt_d / S.rho);
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const Cell cl = tile_cell(my[q], n, lt, m);
+                if (have[q] && cl.ok)
+                    project_cell(S, S.u[par ^ 1], S.v[par ^ 1], S.w[par ^ 1], S.p, x[q * 4 + m], dtr, h, cl);
+            }
+        }
+    }
+finish:
+    if (*(volatile int*)ws.err) {
+        // leave no copy in flight: a timed-out wait is retried (bounded) before the block exits
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) mbar_wait(&mbar[g * MAXC + q], phase_bit ^ 1u);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, false, *(volatile int*)ws.err != 0, par);
 }
 
 const void* pcg_kernel(bool heat) { return heat ? (const void*)k_pcg<true> : (const void*)k_pcg<false>; }
+
+const void* pcg_resident_kernel(bool heat, int maxc, bool tma) {
+    if (heat) {
+        if (maxc == 1) return (const void*)k_pcg_res<true, 1, false>;
+        if (maxc == 2) return (const void*)k_pcg_res<true, 2, false>;
+        return (const void*)k_pcg_res<true, 3, false>;
+    }
+    if (tma) {
+        if (maxc == 1) return (const void*)k_pcg_tma<1>;
+        if (maxc == 2) return (const void*)k_pcg_tma<2>;
+        return (const void*)k_pcg_tma<3>;
+    }
+    if (maxc == 1) return (const void*)k_pcg_res<false, 1, false>;
+    if (maxc == 2) return (const void*)k_pcg_res<false, 2, false>;
+    return (const void*)k_pcg_res<false, 3, false>;
+}
+
+size_t pcg_resident_smem(int groups, int maxc, bool tma) {
+    return tma ? (size_t)groups * maxc * kSlotFloats * sizeof(float) + 128 : 0;
+}
 
 }  // namespace hf

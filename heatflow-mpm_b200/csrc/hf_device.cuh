@@ -25,6 +25,12 @@ struct WorkItem {
     int first;   // first cell (linear index) of the chunk
 };
 
+// CG work item: a 4 x 8 x 32-cell tile (i, j, k) of one scene
+constexpr int kTI = 4, kTJ = 8, kTK = 32;
+struct TileItem {
+    int scene, i0, j0, k0;
+};
+
 // ------------------------------------------------------------------------------------------ lattice arithmetic
 __device__ __forceinline__ int clampi(int i, int lo, int hi) { return i < lo ? lo : (i > hi ? hi : i); }
 __device__ __forceinline__ float minf_(float a, float b) { return a < b ? a : b; }

@@ -1,6 +1,8 @@
 // hf_kernels.cuh -- workspace layout and kernel declarations shared by the kernel files and the host API.
 #pragma once
 
+#include <cuda.h>
+
 #include "hf_device.cuh"
 
 namespace hf {
@@ -18,11 +20,18 @@ struct Workspace {
     unsigned* bar;          // [2] grid-barrier counters (reset before every persistent launch)
     unsigned* live_count;   // [2] scenes still iterating
     int* err;               // [1] barrier timeout flag
-    int* chunk_begin;       // [S+1] first chunk of every scene in the work table
-    CgCtl* ctl;             // [S]
-    unsigned* scene_count;  // [S] chunk arrivals in the current phase (left at 0)
-    double* partials;       // [3*C] per-chunk fp64 partial sums
-    unsigned* diag_bits;    // [4] max-reductions of the diagnostics
+    int* chunk_begin;       // [S+1] first chunk of every scene in the chunk table
+    int* tile_begin;        // [S+1] first tile of every scene in the tile table
+    CgCtl* ctl;             // [S] per-scene CG record written by the scene's owner block
+    double* partA;          // [3*T] per-tile fp64 partials of CG phase A
+    double* partB;          // [3*T] per-tile fp64 partials of the CG set-up and phase B
+    double* mean_part;      // [C] per-chunk fp64 sums of the pressure rhs
+};
+
+// TMA descriptors of the tiled pressure stencil (resident CG): z, both search-direction buffers, alpha_f x (the u
+// lattice), and the cell-layout copies of alpha_f y and z.
+struct TileMaps {
+    CUtensorMap z, p0, p1, ax, ayc, azc;
 };
 
 __global__ void k_scatter(const hf_scene* __restrict__ scenes, int s);
@@ -44,9 +53,11 @@ __global__ void k_heat_matvec_plain(int n, float h, float dt, float alpha, float
                                     const float* __restrict__ kap, const uint8_t* __restrict__ fl,
                                     const float* __restrict__ y, float* __restrict__ out);
 // persistent cooperative Jacobi-PCG kernel (heat = heat system, else pressure system + projection + end of substep);
-// arguments: (const hf_scene*, const WorkItem*, int num_chunks, int num_scenes, double dt, Workspace)
+// arguments: (const hf_scene*, const TileItem*, int num_tiles, int num_scenes, double dt, Workspace)
 const void* pcg_kernel(bool heat);
-// register-resident single-scene variant (MAXC chunks per 256-thread group: 1, 2 or 3); blockDim = 256 x groups
-const void* pcg_resident_kernel(bool heat, int maxc);
+// register-resident single-scene variant (MAXC tiles per 256-thread group: 1, 2 or 3; blockDim = 256 x groups);
+// arguments as pcg_kernel plus a TileMaps (used when tma); dynamic shared memory pcg_resident_smem(...)
+const void* pcg_resident_kernel(bool heat, int maxc, bool tma);
+size_t pcg_resident_smem(int groups, int maxc, bool tma);
 
 }  // namespace hf

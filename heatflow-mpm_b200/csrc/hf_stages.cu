@@ -209,22 +209,25 @@ __global__ void __launch_bounds__(kThreads) k_coeff(const hf_scene* __restrict__
             S.ax[fu] = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
             S.hkx[fu] = face_kappa(conductivity(an, ka, km), kc);
         }
+        float ayv = 0.0f, azv = 0.0f;
         if (j == 0) {
-            S.ay[fv] = 0.0f;
             S.hky[fv] = 0.0f;
         } else {
             const float an = as[t - n];
-            S.ay[fv] = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
+            ayv = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
             S.hky[fv] = face_kappa(conductivity(an, ka, km), kc);
         }
         if (k == 0) {
-            S.az[fw] = 0.0f;
             S.hkz[fw] = 0.0f;
         } else {
             const float an = as[t - 1];
-            S.az[fw] = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
+            azv = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
             S.hkz[fw] = face_kappa(conductivity(an, ka, km), kc);
         }
+        S.ay[fv] = ayv;
+        S.az[fw] = azv;
+        S.ayc[t] = ayv;   // cell-layout copies for the tiled (TMA) pressure stencil
+        S.azc[t] = azv;
         if (i == n - 1) S.ax[uidx(n, n, j, k)] = S.hkx[uidx(n, n, j, k)] = 0.0f;
         if (j == n - 1) S.ay[vidx(n, i, n, k)] = S.hky[vidx(n, i, n, k)] = 0.0f;
         if (k == n - 1) S.az[widx(n, i, j, n)] = S.hkz[widx(n, i, j, n)] = 0.0f;
@@ -462,7 +465,7 @@ __global__ void __launch_bounds__(kThreads) k_divergence(const hf_scene* __restr
         part[0] += (double)r;
     }
     block_sum<1>(part, red);
-    if (threadIdx.x == 0) ws.partials[3 * c] = part[0];
+    if (threadIdx.x == 0) ws.mean_part[c] = part[0];
 }
 
 // ---------------------------------------------------------------------------------------------- diagnostics

@@ -16,6 +16,7 @@ HF_FLAG_BUOYANCY, HF_FLAG_SOURCE, HF_FLAG_PARTICLES, HF_FLAG_ACTIVE = 1, 2, 4, 8
 HF_SCENE_HEAT_MAXITER, HF_SCENE_PRESSURE_MAXITER, HF_SCENE_NONFINITE, HF_SCENE_BARRIER_TIMEOUT = 1, 2, 4, 8
 CHUNK = 1024
 HF_PLAN_STREAMING_CG = 1
+HF_PLAN_NO_TMA = 2
 
 _P = C.c_void_p
 
@@ -44,11 +45,12 @@ class Scene(C.Structure):
                [(f, _P) for f in SCENE_PTRS[:31]] + \
                [("cg_r", _P), ("cg_z", _P), ("cg_p", _P * 2), ("cg_Ap", _P),
                 ("pos", _P), ("pvel", _P), ("ptemp", _P), ("pmelt", _P), ("pyield", _P), ("pvisc", _P),
-                ("hkx", _P), ("hky", _P), ("hkz", _P), ("acc", _P), ("state", _P)]
+                ("hkx", _P), ("hky", _P), ("hkz", _P), ("ayc", _P), ("azc", _P), ("acc", _P), ("state", _P)]
 
 
 class Plan(C.Structure):
-    _fields_ = [("num_scenes", C.c_int32), ("num_chunks", C.c_int32), ("scenes_host", _P), ("scenes_dev", _P),
+    _fields_ = [("num_scenes", C.c_int32), ("num_chunks", C.c_int32), ("num_tiles", C.c_int32), ("reserved_t", C.c_int32),
+                ("tiles_dev", _P), ("scenes_host", _P), ("scenes_dev", _P),
                 ("work_dev", _P), ("workspace", _P), ("workspace_bytes", C.c_size_t), ("persistent_blocks", C.c_int32),
                 ("options", C.c_int32)]
 
@@ -70,8 +72,9 @@ def load():
     L = C.CDLL(LIB_PATH)
     L.hf_last_error.restype = C.c_char_p
     L.hf_workspace_bytes.restype = C.c_size_t
-    L.hf_workspace_bytes.argtypes = [C.c_int, C.c_int]
+    L.hf_workspace_bytes.argtypes = [C.c_int, C.c_int, C.c_int]
     L.hf_chunks_for.argtypes = [C.c_int]
+    L.hf_tiles_for.argtypes = [C.c_int]
     L.hf_plan_upload.argtypes = [C.POINTER(Plan), _P]
     for name in ("hf_temperature_stage", "hf_heat_solve", "hf_face_stage", "hf_pressure_solve", "hf_substep",
                  "hf_divergence_stage", "hf_pressure_cg"):

@@ -82,6 +82,7 @@ class DeviceScene:
         self.cg_p = [z(n, n, n), z(n, n, n)]
         self.ax, self.ay, self.az = (z(*s) for s in fs)
         self.hk = [z(*s) for s in fs]
+        self.ayc, self.azc = z(n, n, n), z(n, n, n)
         self.cell_flags = z(n, n, n, dtype=torch.uint8)
         coupled = spec.n_particles > 0
         has_static = spec.static_alpha is not None
@@ -188,6 +189,7 @@ class DeviceScene:
         r.cg_p[0], r.cg_p[1] = P(s.cg_p[0]), P(s.cg_p[1])
         r.pos, r.pvel, r.ptemp, r.pmelt, r.pyield, r.pvisc = (P(a) for a in (s.pos, s.pvel, s.ptemp, s.pmelt, s.pyield, s.pvisc))
         r.hkx, r.hky, r.hkz = (P(a) for a in s.hk)
+        r.ayc, r.azc = P(s.ayc), P(s.azc)
         r.acc = P(s.acc)
         r.state = P(s.state)
 
@@ -212,7 +214,7 @@ class DeviceScene:
 class ScenePlan:
     """Scene table + work table + workspace for a list of DeviceScene, and the stage calls over them."""
 
-    def __init__(self, scenes, device="cuda:0", persistent_blocks=0, streaming_cg=False):
+    def __init__(self, scenes, device="cuda:0", persistent_blocks=0, streaming_cg=False, tma=True):
         self.L = _lib.load()
         self.scenes = list(scenes)
         self.device = torch.device(device)
@@ -221,19 +223,22 @@ class ScenePlan:
         for i, sc in enumerate(self.scenes):
             self.host[i] = sc.record
         C_total = sum(self.L.hf_chunks_for(sc.n) for sc in self.scenes)
+        T_total = sum(self.L.hf_tiles_for(sc.n) for sc in self.scenes)
         self.scenes_dev = torch.zeros(C.sizeof(_lib.Scene) * S, dtype=torch.uint8, device=self.device)
         self.work_dev = torch.zeros(2 * max(C_total, 1), dtype=torch.int32, device=self.device)
-        ws_bytes = self.L.hf_workspace_bytes(S, C_total)
+        self.tiles_dev = torch.zeros(4 * max(T_total, 1), dtype=torch.int32, device=self.device)
+        ws_bytes = self.L.hf_workspace_bytes(S, C_total, T_total)
         self.workspace = torch.zeros(ws_bytes, dtype=torch.uint8, device=self.device)
         self.plan = _lib.Plan()
         self.plan.num_scenes = S
         self.plan.scenes_host = C.cast(self.host, C.c_void_p)
         self.plan.scenes_dev = self.scenes_dev.data_ptr()
         self.plan.work_dev = self.work_dev.data_ptr()
+        self.plan.tiles_dev = self.tiles_dev.data_ptr()
         self.plan.workspace = self.workspace.data_ptr()
         self.plan.workspace_bytes = ws_bytes
         self.plan.persistent_blocks = persistent_blocks
-        self.plan.options = _lib.HF_PLAN_STREAMING_CG if streaming_cg else 0
+        self.plan.options = (_lib.HF_PLAN_STREAMING_CG if streaming_cg else 0) | (0 if tma else _lib.HF_PLAN_NO_TMA)
         self.upload()
 
     def stream(self):

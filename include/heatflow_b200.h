@@ -102,6 +102,8 @@ typedef struct hf_scene {
     float *pos, *pvel, *ptemp, *pmelt, *pyield, *pvisc;
     /* harmonic face diffusivities 2 k_a k_b / (k_a + k_b + 1e-12) of the three face lattices (heat.py:50-52) */
     float *hkx, *hky, *hkz;
+    /* alpha_f of the low y and z face of every cell in cell layout (n,n,n) (copies of ay, az for tiled loads) */
+    float *ayc, *azc;
     /* 12 fixed-point accumulators of (n+1)^3 int64 each (coupled scenes only), zero on entry, left zero */
     long long *acc;
     hf_scene_state *state;
@@ -109,12 +111,16 @@ typedef struct hf_scene {
 
 /* hf_plan.options */
 #define HF_PLAN_STREAMING_CG 1u      /* never use the register-resident CG variant (single-scene plans use it when
-                                        the scene's chunks fit one block per SM) */
+                                        the scene's tiles fit one block per SM) */
+#define HF_PLAN_NO_TMA 2u            /* resident pressure CG without the TMA-staged stencil */
 
 /* A batch of scenes ready to launch: tables in device memory plus the host copy used to size launches. */
 typedef struct hf_plan {
     int32_t num_scenes;
     int32_t num_chunks;        /* 1024-cell work items over all scenes */
+    int32_t num_tiles;         /* 4 x 8 x 32-cell tiles over all scenes (work items of the CG solves) */
+    int32_t reserved_t;
+    void *tiles_dev;           /* device: int32 quadruples (scene, i0, j0, k0) [num_tiles] */
     const hf_scene *scenes_host;   /* host copy, valid while the plan is used */
     void *scenes_dev;          /* device: hf_scene[num_scenes] */
     void *work_dev;            /* device: int32 pairs (scene, first cell) [num_chunks] */
@@ -128,11 +134,12 @@ typedef struct hf_plan {
 int hf_abi_version(void);
 const char *hf_last_error(void);
 int hf_cells_per_chunk(void);
-/* workspace bytes for a plan of num_scenes scenes and num_chunks chunks */
-size_t hf_workspace_bytes(int num_scenes, int num_chunks);
-/* number of 1024-cell chunks of a scene of n cells per edge */
+/* workspace bytes for a plan of num_scenes scenes, num_chunks chunks and num_tiles tiles */
+size_t hf_workspace_bytes(int num_scenes, int num_chunks, int num_tiles);
+/* number of 1024-cell chunks / 4x8x32 tiles of a scene of n cells per edge */
 int hf_chunks_for(int n);
-/* Writes the scene table and the work table to the device and fills plan.num_chunks.  Blocking: the stream is
+int hf_tiles_for(int n);
+/* Writes the scene table and the chunk and tile work tables to the device and fills plan.num_chunks/num_tiles.  Blocking: the stream is
  * synchronised before return (set-up call, not for the per-substep path). */
 int hf_plan_upload(hf_plan *plan, void *stream);
 

@@ -42,7 +42,8 @@ def test_pure_functions_without_gpu():
     assert L.hf_abi_version() == 1
     assert L.hf_cells_per_chunk() == 1024
     assert L.hf_chunks_for(96) == 864 and L.hf_chunks_for(10) == 1
-    assert L.hf_workspace_bytes(1, 864) > 3 * 8 * 864
+    assert L.hf_tiles_for(96) == 864 and L.hf_tiles_for(48) == 144
+    assert L.hf_workspace_bytes(1, 864, 864) > 6 * 8 * 864
 
 
 def test_record_layout_matches_header(tmp_path):
