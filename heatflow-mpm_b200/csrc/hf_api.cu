@@ -233,6 +233,16 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
 
 }  // namespace
 
+namespace hf {
+int set_error(int code, const char* msg) { return fail(code, msg); }
+
+void plan_offset_tables(const hf_plan* p, int** chunk_begin, int** tile_begin) {
+    const Workspace w = workspace(p);
+    *chunk_begin = w.chunk_begin;
+    *tile_begin = w.tile_begin;
+}
+}  // namespace hf
+
 extern "C" {
 
 int hf_abi_version(void) { return HF_ABI_VERSION; }

@@ -59,5 +59,9 @@ const void* pcg_kernel(bool heat);
 // arguments as pcg_kernel plus a TileMaps (used when tma); dynamic shared memory pcg_resident_smem(...)
 const void* pcg_resident_kernel(bool heat, int maxc, bool tma);
 size_t pcg_resident_smem(int groups, int maxc, bool tma);
+// device addresses of the per-scene chunk and tile offset tables inside a plan's workspace
+void plan_offset_tables(const hf_plan* p, int** chunk_begin, int** tile_begin);
+// record `msg` as the text of hf_last_error() and return `code`
+int set_error(int code, const char* msg);
 
 }  // namespace hf

@@ -184,6 +184,24 @@ int hf_k_laplacian(int n, double h, double alpha, double beta, const float *p, c
 int hf_k_heat_matvec(int n, double h, double dt, double alpha, double beta, const float *x, const float *kap,
                      const uint8_t *cell_flags, const float *y, float *out, void *stream);
 
+/* ------------------------------------------------------------------------------------ without device allocation */
+/* No counterpart in the reference: an entry point for callers that cannot allocate device memory (code running where
+ * no allocator may be called -- inside an allocator callback, under a memory budget owned by someone else, or in a
+ * host that plans all device memory up front).  It performs hf_pressure_solve for ONE scene of edge n <= 64
+ * (hf_noalloc_max_edge()): divergence of the face velocities, mean removal, Jacobi-PCG warm-started from p, and the
+ * projection of u, v, w in place.  The caller passes the inputs and outputs only (reference layouts; qx/qy/qz may all
+ * be NULL for zero solid flux); the scene record, work tables, CG workspace and CG vectors live in a fixed file-scope
+ * device array of hf_noalloc_scratch_bytes() bytes (9 MiB) that every GPU loading the library holds until exit.
+ * No cudaMalloc/cudaFree or allocating library call is made.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls on a device share the array: calls whose
+ * GPU work overlaps race; each call clears what must start at zero.  state_out (device, optional) receives the solve
+ * statistics.  Returns HF_ERR_ARG for n > 64. */
+size_t hf_noalloc_scratch_bytes(void);
+int hf_noalloc_max_edge(void);
+int hf_pressure_solve_noalloc(int n, double h, double rho, double dt, double cg_tol, int cg_max_iter, float *u, float *v,
+                              float *w, const float *ax, const float *ay, const float *az, const float *qx,
+                              const float *qy, const float *qz, float *p, hf_scene_state *state_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
