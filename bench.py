@@ -1,19 +1,32 @@
-"""Benchmark: 96^3 air substeps/s of Heatflow-MPM's Eulerian air path on B200.
+"""Benchmark: 96^3 air substeps/s of Heatflow-MPM's Eulerian air path on B200, plain and batched-served.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload plain|batched|served]
 
-Workload (every arm): the default coupled 96^3 scene -- h = 5 mm, trough heater 400 W capped at 120 C, fan 2 m/s,
-rods 300 C, room 25 C, a seeded ellipsoid of ~16k particles (semi-axes 4/3/5 cm, 2.5 mm jittered lattice) at 20 C,
-melt law T_sol 28 / T_liq 34; pressure CG tol 1e-4 (maxiter 400), heat CG tol 1e-6 (maxiter 200); dt = 2 ms.  Newton
-(the material solver) is not installed, so the particles keep their positions and velocities (frozen body); the air
+plain (default line) -- the default coupled 96^3 scene: h = 5 mm, trough heater 400 W capped at 120 C, fan 2 m/s, rods
+300 C, room 25 C, a seeded ellipsoid of ~16k particles (semi-axes 4/3/5 cm, 2.5 mm jittered lattice) at 20 C, melt
+law T_sol 28 / T_liq 34; pressure CG tol 1e-4 (maxiter 400), heat CG tol 1e-6 (maxiter 200); dt = 2 ms.  Newton (the
+material solver) is not installed, so the particles keep their positions and velocities (frozen body); the air
 substep still scatters them, rebuilds the obstacle fields and updates their temperatures every substep.  Both arms
-start from the state after a deterministic spin-up of --spinup substeps from the initial scene (the CUDA path and the
-CPU port reach the same state: they agree bit for bit), then W warm-up substeps, then K timed substeps.
+start from the state after a deterministic spin-up of --spinup substeps, then W warm-up substeps, then K timed
+substeps.  `value` = substeps/s with the state resident in HBM (CUDA events on the stream, barrier + synchronize on both
+sides, max over ranks); `e2e` = the same through the public API with the particle state copied from pinned host memory
+before and the grid temperature copied back after every substep.
 
-A step is one air substep.  `value` = substeps/s with the state resident in HBM (timed with CUDA events on the stream,
-barrier + synchronize on both sides, max over ranks); `e2e` = the same through the public API with the particle state
-copied from pinned host memory before and the grid temperature copied back after every substep.  The CPU reference
-arm (--impl reference) times the CPU port of the reference's algorithm (oracle/) on the host cores.
+batched -- 64 air-only scenes (edge drawn from {32,48,64,96,128}, h = 0.48 m / edge, box heater at x U(0.05,0.2) m,
+power U(100,800) W, fan U(0,3) m/s; seeded), one launch per stage per substep for the whole batch, K substeps replayed
+from a CUDA graph of --graph-steps substeps.  value = 96^3-equivalent substeps/s (cells x substeps / 96^3 / s).
+
+served -- Poisson arrivals (--rate per s, default 20) of air scenarios (edge from {48,64,96,128}, horizon U(200,2000)
+substeps, power U(100,800) W, fan U(0,3) m/s, with probability 1/2 a static solid sphere of radius U(2,6) cm held at
+20 C), admitted against an HBM budget and continuously batched, for --serve-seconds of wall clock.  value = 96^3-
+equivalent substeps/s while the GPU computes (sum of the batched substeps' CUDA-event times); e2e = the same work over
+the wall-clock window (admission, scene upload, plan rebuilds, result download included); p50/p99 of request and
+batched-substep latency.
+
+The default line carries compact `batched` and `served` summaries (--no-extras drops them).  The CPU reference arm
+(--impl reference) times the CPU port of the reference's algorithm (oracle/) on the host cores, plain workload.
+Multi-GPU: plain runs one replica per GPU; batched and served shard whole scenes (requests) across GPUs, no collective
+on the data path.
 """
 from __future__ import annotations
 
@@ -34,26 +47,70 @@ import numpy as np  # noqa: E402
 
 DT = 2.0e-3
 METRIC = "96^3 air substeps/s (default coupled scene, plain path)"
+METRIC_BATCHED = "96^3-equivalent air substeps/s (64-scene batched ensemble)"
+METRIC_SERVED = "96^3-equivalent air substeps/s (served Poisson trace, continuous batching)"
 PUBLISHED_SUBSTEPS_PER_S = 1000.0 / 7.0   # README.md:46 of the reference: ~7 ms per air substep (RTX 5080)
 WORKLOAD = ("default coupled scene 96^3 (h=5 mm, 400 W cap 120 C, fan 2 m/s, ~16k-particle ellipsoid, frozen body), "
             "dt=2 ms, pressure tol 1e-4, heat tol 1e-6")
+N96 = 96 ** 3
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=None, help="timed substeps (plain 1000, batched 200)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served"])
     ap.add_argument("--spinup", type=int, default=30, help="substeps from the initial scene before warm-up (both arms)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=60.0, help="budget of the timed CPU reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="plain line without the batched/served summaries")
+    ap.add_argument("--scenes", type=int, default=64, help="batched: scenes in the ensemble")
+    ap.add_argument("--graph-steps", type=int, default=10, help="batched: substeps per captured CUDA graph")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="served: length of the trace window")
+    ap.add_argument("--rate", type=float, default=20.0, help="served: mean arrivals per second")
+    ap.add_argument("--hbm-budget", type=float, default=150e9, help="served: HBM admitted for scenes, bytes")
+    ap.add_argument("--max-slots", type=int, default=256, help="served: most scenes in one batch")
     return ap.parse_args()
 
 
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def _reduce(x, op, dev, world):
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
+def reduce_max(x, dev, world):
+    import torch.distributed as dist
+    return _reduce(x, dist.ReduceOp.MAX if world > 1 else None, dev, world)
+
+
+def reduce_sum(x, dev, world):
+    import torch.distributed as dist
+    return _reduce(x, dist.ReduceOp.SUM if world > 1 else None, dev, world)
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def load_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
 
 
 # --------------------------------------------------------------------------------------------------- CPU side
@@ -89,18 +146,40 @@ def time_cpu_substeps(sc, budget_s, max_steps, min_steps=1):
     return done, time.perf_counter() - t0
 
 
+def cpu_scenarios_sample(scenarios, budget_s, per_scene=2):
+    """CPU port on air scenarios, per_scene substeps each from their initial state, in order, until budget_s:
+    returns (96^3-equivalent substeps/s, substeps done, scenes visited, seconds)."""
+    from oracle import oracle as O
+    O.set_threads(host_threads())
+    cells, done, visited, el = 0, 0, 0, 0.0
+    for sc in scenarios:
+        if el > budget_s:
+            break
+        o = O.scene_from_spec(sc.spec(), "f32")
+        o.set_state(T=np.where(sc.spec().fixed, sc.spec().tfix, sc.initial_T()).astype(np.float32))
+        t0 = time.perf_counter()
+        for _ in range(per_scene):
+            o.substep(DT)
+        el += time.perf_counter() - t0
+        cells += per_scene * sc.n ** 3
+        done += per_scene
+        visited += 1
+    return cells / N96 / el, done, visited, el
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
     from oracle import oracle as O
     O.set_threads(host_threads())
+    steps = args.steps if args.steps is not None else 1000
     sc, spec = cpu_scene()
     t0 = time.perf_counter()
     for _ in range(args.spinup + args.warmup):
         sc.substep(DT)
     t_setup = time.perf_counter() - t0
-    done, el = time_cpu_substeps(sc, budget_s=args.ref_seconds, max_steps=args.steps, min_steps=min(3, args.steps))
+    done, el = time_cpu_substeps(sc, budget_s=args.ref_seconds, max_steps=steps, min_steps=min(3, steps))
     v = done / el
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "substeps/s", "n_gpus": args.gpus,
            "steps": done, "warmup": args.warmup, "ms_per_step": 1000.0 * el / done, "higher_is_better": True,
@@ -108,7 +187,7 @@ def run_reference(args):
            "data": "synthetic (seeded ellipsoid particles, reference heater geometry)",
            "config": {"workload": WORKLOAD, "spinup": args.spinup, "n": spec.n, "cells": spec.n ** 3},
            "cpu_baseline": {"value": v, "unit": "substeps/s", "cores": O.num_threads(), "kind": "port",
-                            "sample": f"{done} substeps (of --steps {args.steps}, bounded to {args.ref_seconds:.0f} s) of the "
+                            "sample": f"{done} substeps (of --steps {steps}, bounded to {args.ref_seconds:.0f} s) of the "
                                       f"workload on the CPU port (oracle/hf_oracle.c, OpenMP), after "
                                       f"{args.spinup}+{args.warmup} untimed substeps ({t_setup:.0f} s)"},
            "e2e": {"value": v, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -162,7 +241,7 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# --------------------------------------------------------------------------------------------------- GPU side
+# --------------------------------------------------------------------------------------------------- bytes
 def pressure_bytes_per_launch(N, iters):
     """Algorithmic bytes of one pressure-solve launch: 52 N per CG iteration (matvec 20 N + vector update 32 N),
     36 N of set-up (read rhs, p, alpha_f x3; write rhs, diag, r, z) and 28 N for the projection (read u,v,w,p;
@@ -170,21 +249,26 @@ def pressure_bytes_per_launch(N, iters):
     return (52.0 * iters + 36.0 + 28.0) * N
 
 
-def main():
-    args = parse()
-    if args.impl == "reference":
-        run_reference(args)
-        return
+def substep_bytes(N, it_heat, it_pressure, coupled):
+    """Algorithmic bytes of one whole air substep: 158 N + 45 N per heat CG iteration + 52 N per pressure CG iteration
+    (air-only; statics counted once per scene), +32 N when particles rebuild the obstacle fields (T pre-stage +8 N,
+    heat rhs +12 N, divergence +12 N)."""
+    return (158.0 + (32.0 if coupled else 0.0) + 45.0 * it_heat + 52.0 * it_pressure) * N
+
+
+def roofline(achieved_gbs, peaks, **extra):
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    out = {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s", "frac": achieved_gbs / peak,
+           "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    out.update(extra)
+    return out
+
+
+# --------------------------------------------------------------------------------------------------- plain
+def bench_plain(args, dev, rank, world, local):
     import torch
-    import torch.distributed as dist
-    from heatflow_mpm import _lib
     from heatflow_mpm.synthetic import coupled_default
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    dev = f"cuda:{local}"
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    steps = args.steps if args.steps is not None else 1000
     sim = coupled_default(device=dev)
     sc, plan = sim.scene, sim.plan
     n = sim.grid.n
@@ -198,15 +282,14 @@ def main():
     p_at_start = sc.p.cpu().numpy().copy()
     ptemp_at_start = sc.ptemp.cpu().numpy().copy()
     # ---- timed region: K substeps, stage by stage, events around every pressure-solve launch
-    pe = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    pe = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
-    if world > 1:
-        dist.barrier()
+    barrier(world)
     torch.cuda.synchronize()
     clocks.start()
     t_start.record(stream)
-    for s in range(args.steps):
+    for s in range(steps):
         plan.obstacle_fields()
         plan.temperature_stage(DT)
         plan.heat_solve(DT)
@@ -219,57 +302,45 @@ def main():
     t_end.record(stream)
     torch.cuda.synchronize()
     ck = clocks.stop()
-    el_ms = t_start.elapsed_time(t_end)
-    if world > 1:
-        t = torch.tensor([el_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el_ms = float(t.item())
+    el_ms = reduce_max(t_start.elapsed_time(t_end), dev, world)
     st1 = sc.read_state()
     p_iters = int(st1.total_pressure_iters - st0.total_pressure_iters)
     h_iters = int(st1.total_heat_iters - st0.total_heat_iters)
     cg_ms = sum(a.elapsed_time(b) for a, b in pe)
-    value = world * args.steps / (el_ms / 1000.0)
-    launches_per_step = 10   # scatter, obstacle, coeff, prestage, advect_T, heat CG, particle update, face, divergence, pressure CG
+    value = world * steps / (el_ms / 1000.0)
+    # footprint, scatter, obstacle, coeff, prestage, advect_T, heat CG, particle update, face, divergence, pressure CG
+    launches_per_step = 11
     # ---- end to end through the public API: pinned H2D of the particle state, D2H of grid_T, every substep
     pos_h = sim.body.pos_t.cpu().pin_memory()
     vel_h = sim.body.vel_t.cpu().pin_memory()
     out_h = torch.empty((n, n, n), dtype=torch.float32).pin_memory()
-    if world > 1:
-        dist.barrier()
+    barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         sim.body.set_state(pos_h, vel_h)
         sim.substep(DT)
         sim.grid_T(out=out_h)
         torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * args.steps / e2e_s, "unit": "substeps/s",
+    e2e_s = reduce_max(time.perf_counter() - t0, dev, world)
+    e2e = {"value": world * steps / e2e_s, "unit": "substeps/s",
            "h2d_bytes_per_step": int(pos_h.numel() * 4 + vel_h.numel() * 4), "d2h_bytes_per_step": int(out_h.numel() * 4)}
-    # ---- roofline of the dominant kernel (pressure CG + projection)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    cg_bytes = pressure_bytes_per_launch(N, p_iters / args.steps)
-    achieved = cg_bytes / (cg_ms / args.steps / 1000.0) / 1e9
+    # ---- roofline of the dominant kernel (pressure CG + projection) and of the whole substep
+    peaks = load_peaks()
+    cg_bytes = pressure_bytes_per_launch(N, p_iters / steps)
     traffic = None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "pressure_cg_96.json")))
-        traffic = prof["dram_bytes_per_iteration"] * (p_iters / args.steps) + prof.get("dram_bytes_fixed", 0.0)
+        traffic = prof["dram_bytes_per_iteration"] * (p_iters / steps) + prof.get("dram_bytes_fixed", 0.0)
     except (OSError, ValueError, KeyError):
         pass
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-            "kernel": "k_pcg<pressure> (Jacobi-PCG + projection, persistent cooperative)",
-            "bytes_per_launch": cg_bytes, "ms_per_launch": cg_ms / args.steps,
-            "mean_pressure_iters": p_iters / args.steps}
+    roof = roofline(cg_bytes / (cg_ms / steps / 1000.0) / 1e9, peaks, traffic=traffic,
+                    kernel="k_pcg_tma<1> (pressure Jacobi-PCG + projection, one persistent cooperative launch, "
+                           "TMA-staged register-resident stencil)",
+                    bytes_per_launch=cg_bytes, ms_per_launch=cg_ms / steps, mean_pressure_iters=p_iters / steps)
+    sb = substep_bytes(N, h_iters / steps, p_iters / steps, True)
+    sub_gbs = sb / (el_ms / steps / 1000.0) / 1e9
+    sub_roof = {"bytes_per_substep": sb, "achieved": sub_gbs, "unit": "GB/s", "frac": sub_gbs / roof["peak"]}
     # ---- CPU baseline: the CPU port from the same state, bounded sample (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -279,22 +350,221 @@ def main():
         osc.set_state(T=state_at_start["T"], u=state_at_start["u"], v=state_at_start["v"], w=state_at_start["w"])
         osc.a["p"][...] = p_at_start
         osc.a["ptemp"][: len(ptemp_at_start)] = ptemp_at_start
-        done, el = time_cpu_substeps(osc, args.cpu_seconds, max_steps=args.steps)
+        done, el = time_cpu_substeps(osc, args.cpu_seconds, max_steps=steps)
         cpu = {"value": done / el, "unit": "substeps/s", "cores": O.num_threads(), "kind": "port",
                "sample": f"{done} substeps of the same workload from the same state on the CPU port "
                          f"(oracle/hf_oracle.c, OpenMP {O.num_threads()} threads), {el:.1f} s"}
+    return {"metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": el_ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / PUBLISHED_SUBSTEPS_PER_S, "dtype": "f32",
+            "data": "synthetic (seeded ellipsoid particles, reference heater geometry)",
+            "config": {"workload": WORKLOAD, "n": n, "cells": N, "spinup": args.spinup, "parallelism": f"replicas x{world}",
+                       "l2": "scene state ~170 MB > 126 MB L2 (inputs larger than L2); the CG working set "
+                             "(~35 MB) stays L2-resident within a substep by design",
+                       "mean_pressure_iters": p_iters / steps, "mean_heat_iters": h_iters / steps,
+                       "cell_updates_per_s": value * N, "substep_status": int(st1.status),
+                       "substep_roofline": sub_roof},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * steps, "clocks": ck}
+
+
+# --------------------------------------------------------------------------------------------------- batched
+def bench_batched(args, dev, rank, world, local, steps, warmup, cpu_sample=True):
+    import torch
+    from heatflow_mpm.batch import AirBatch, autotune, ensemble, shard_scenarios
+    scs_all = ensemble(count=args.scenes, seed=0, steps=steps)
+    mine = shard_scenarios(scs_all, rank, world)
+    t_build = time.perf_counter()
+    batch = AirBatch(mine, device=dev)
+    t_build = time.perf_counter() - t_build
+    pb, tune = autotune(batch, dt=DT, reps=2)
+    for _ in range(warmup):
+        batch.substep(DT)
+    G = max(1, min(args.graph_steps, steps))
+    batch.capture(DT, G)
+    torch.cuda.synchronize()
+    st0 = batch.states()
+    stream = torch.cuda.current_stream()
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start.record(stream)
+    for _ in range(steps // G):
+        batch.graph.replay()
+    for _ in range(steps % G):
+        batch.substep(DT)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    el_ms = reduce_max(t_start.elapsed_time(t_end), dev, world)
+    st1 = batch.states()
+    cells_mine = sum(s.n ** 3 for s in mine)
+    cells = reduce_sum(cells_mine, dev, world)
+    value = cells * steps / N96 / (el_ms / 1000.0)
+    it_p = [(b.total_pressure_iters - a.total_pressure_iters) / steps for a, b in zip(st0, st1)]
+    it_h = [(b.total_heat_iters - a.total_heat_iters) / steps for a, b in zip(st0, st1)]
+    sb_mine = sum(substep_bytes(s.n ** 3, h, p, False) for s, h, p in zip(mine, it_h, it_p))
+    sb = reduce_sum(sb_mine, dev, world)
+    status = [int(s.status) for s in st1]
+    # ---- stage breakdown (eager, outside the timed region): events around the pressure-CG launch of the batch
+    B = 10
+    pe = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(B)]
+    sa = batch.states()
+    plan = batch.plan
+    for k in range(B):
+        plan.temperature_stage(DT)
+        plan.heat_solve(DT)
+        plan.face_stage(DT)
+        plan.divergence_stage(DT)
+        pe[k][0].record(stream)
+        plan.pressure_cg(DT)
+        pe[k][1].record(stream)
+    torch.cuda.synchronize()
+    sbk = batch.states()
+    cg_ms = sum(a.elapsed_time(b) for a, b in pe) / B
+    cg_bytes = sum(pressure_bytes_per_launch(s.n ** 3, (b.total_pressure_iters - a.total_pressure_iters) / B)
+                   for s, a, b in zip(mine, sa, sbk))
+    peaks = load_peaks()
+    roof = roofline(cg_bytes / (cg_ms / 1000.0) / 1e9, peaks, traffic=None,
+                    kernel="k_pcg<0> (streaming persistent pressure Jacobi-PCG + projection over the scene table)",
+                    bytes_per_launch=cg_bytes, ms_per_launch=cg_ms, measured_on="rank 0 stage breakdown, 10 substeps")
+    sub_gbs = sb / (el_ms / steps / 1000.0) / 1e9
+    # ---- end to end through the public API: AirBatch.substep per substep, every scene's status block read back
+    state_h = torch.empty((len(batch.scenes), batch.scenes[0].state.numel()), dtype=torch.uint8).pin_memory()
+    e2e_steps = min(steps, 50)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        batch.substep(DT)
+        for i, s in enumerate(batch.scenes):
+            state_h[i].copy_(s.state, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = reduce_max(time.perf_counter() - t0, dev, world)
+    e2e = {"value": cells * e2e_steps / N96 / e2e_s, "unit": "96^3-equivalent substeps/s", "h2d_bytes_per_step": 0,
+           "d2h_bytes_per_step": int(state_h.numel()), "steps": e2e_steps,
+           "note": "AirBatch.substep (eager, no graph) + every scene's state block copied to pinned host memory"}
+    cpu = None
+    if cpu_sample and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        v, done, visited, el = cpu_scenarios_sample(scs_all, args.cpu_seconds)
+        cpu = {"value": v, "unit": "96^3-equivalent substeps/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"{done} substeps: the ensemble's first {visited} scenes, 2 substeps each from their initial "
+                         f"state, on the CPU port (oracle/hf_oracle.c, OpenMP), {el:.1f} s"}
+    hist = {}
+    for s in scs_all:
+        hist[s.n] = hist.get(s.n, 0) + 1
+    return {"metric": METRIC_BATCHED, "value": value, "unit": "96^3-equivalent substeps/s", "n_gpus": world,
+            "steps": steps, "warmup": warmup, "ms_per_step": el_ms / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded ensemble of air-only box-heater scenes)",
+            "config": {"workload": f"batched ensemble: {args.scenes} air-only scenes, edges {dict(sorted(hist.items()))}, "
+                                   f"h=0.48 m/edge, box heater x U(0.05,0.2) m, 100-800 W, fan 0-3 m/s, dt=2 ms, "
+                                   f"pressure tol 1e-4, heat tol 1e-6",
+                       "scenes": args.scenes, "cells": int(cells), "graph_substeps": G, "persistent_blocks": pb,
+                       "autotune_ms": tune, "parallelism": f"scene-sharded x{world}",
+                       "l2": f"{cells * 4 * 40 / 1e9:.1f} GB of scene state > 126 MB L2 (inputs larger than L2)",
+                       "scene_substeps_per_s": len(scs_all) * steps / (el_ms / 1000.0),
+                       "cell_updates_per_s": cells * steps / (el_ms / 1000.0),
+                       "mean_pressure_iters": float(np.mean(it_p)), "mean_heat_iters": float(np.mean(it_h)),
+                       "status_nonzero": int(sum(1 for x in status if x)), "build_s": t_build,
+                       "substep_roofline": {"bytes_per_substep": sb, "achieved": sub_gbs, "unit": "GB/s",
+                                            "frac": sub_gbs / roof["peak"]}},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 6 * steps, "clocks": ck}
+
+
+# --------------------------------------------------------------------------------------------------- served
+def bench_served(args, dev, rank, world, local, cpu_sample=True):
+    import torch
+    from heatflow_mpm.serve import AirServer, poisson_trace
+    trace_all = poisson_trace(rate=args.rate, duration=args.serve_seconds, seed=0)
+    trace = [r for r in trace_all if r.rid % world == rank]
+    srv = AirServer(device=dev, dt=DT, hbm_budget=args.hbm_budget, max_slots=args.max_slots)
+    # warm-up: one small request served to completion (module loading, kernel attributes), not counted
+    from heatflow_mpm.batch import AirScenario
+    from heatflow_mpm.serve import Request
+    warm = AirServer(device=dev, dt=DT)
+    warm.serve([Request(AirScenario(n=48, horizon=max(3, args.warmup)), 0.0)], time_limit=120.0)
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    out = srv.serve(trace, time_limit=args.serve_seconds)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    busy_s = reduce_max(sum(srv.substep_ms) / 1000.0, dev, world)
+    wall_s = reduce_max(srv.elapsed, dev, world)
+    work = reduce_sum(srv.weighted_substeps, dev, world)
+    scene_substeps = reduce_sum(srv.scene_substeps, dev, world)
+    steps = max(1, len(srv.substep_ms))
+    cpu = None
+    if cpu_sample and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        v, done, visited, el = cpu_scenarios_sample([r.scenario for r in trace_all], args.cpu_seconds)
+        cpu = {"value": v, "unit": "96^3-equivalent substeps/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"{done} substeps: the trace's first {visited} requests, 2 substeps each from their initial "
+                         f"state, on the CPU port (oracle/hf_oracle.c, OpenMP), {el:.1f} s"}
+    return {"metric": METRIC_SERVED, "value": work / busy_s, "unit": "96^3-equivalent substeps/s", "n_gpus": world,
+            "steps": len(srv.substep_ms), "warmup": max(3, args.warmup), "ms_per_step": 1000.0 * busy_s / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Poisson trace of air-only trough-heater scenes, half with a static sphere)",
+            "config": {"workload": f"served: Poisson arrivals {args.rate}/s for {args.serve_seconds:.0f} s, edges "
+                                   f"{{48,64,96,128}}, horizon U(200,2000), 100-800 W, fan 0-3 m/s, sphere r U(2,6) cm "
+                                   f"p=0.5, HBM budget {args.hbm_budget / 1e9:.0f} GB, max {args.max_slots} scenes/batch",
+                       "requests": len(trace_all), "requests_done": int(reduce_sum(out["requests_done"], dev, world)),
+                       "requests_unfinished": int(reduce_sum(out["requests_unfinished"], dev, world)),
+                       "request_latency_p50_s": out["request_latency_p50_s"],
+                       "request_latency_p99_s": out["request_latency_p99_s"],
+                       "substep_latency_p50_ms": out["substep_latency_p50_ms"],
+                       "substep_latency_p99_ms": out["substep_latency_p99_ms"],
+                       "scene_substeps": int(scene_substeps), "plan_builds": out["plan_builds"],
+                       "gpu_busy_frac": busy_s / wall_s, "parallelism": f"request-sharded x{world}",
+                       "latency_note": "request latency = arrival to last substep, over completed requests (rank 0)",
+                       "l2": "resident scene state of the admitted requests >> 126 MB L2"},
+            "roofline": None, "cpu_baseline": cpu,
+            "e2e": {"value": work / wall_s, "unit": "96^3-equivalent substeps/s",
+                    "h2d_bytes_per_step": int(srv.h2d_bytes / steps), "d2h_bytes_per_step": int(srv.d2h_bytes / steps),
+                    "note": "wall clock of the serving window: admission, scene upload, plan rebuilds and result "
+                            "download (T of every completed request) included"},
+            "gpu_launches": 6 * len(srv.substep_ms), "clocks": ck}
+
+
+def compact(line):
+    keep = ("value", "unit", "ms_per_step", "steps", "e2e", "cpu_baseline", "clocks")
+    out = {k: line.get(k) for k in keep}
+    out["roofline_frac"] = (line.get("roofline") or {}).get("frac")
+    out["config"] = line.get("config")
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.workload == "plain":
+        out = bench_plain(args, dev, rank, world, local)
+        if not args.no_extras:
+            b = bench_batched(args, dev, rank, world, local, steps=200, warmup=3, cpu_sample=False)
+            out["batched"] = compact(b)
+            out["batched"]["plain_ratio"] = b["value"] / out["value"]
+            out["served"] = compact(bench_served(args, dev, rank, world, local, cpu_sample=False))
+            out["served"]["plain_ratio"] = out["served"]["value"] / out["value"]
+    elif args.workload == "batched":
+        out = bench_batched(args, dev, rank, world, local, args.steps if args.steps is not None else 200,
+                            max(3, args.warmup))
+    else:
+        out = bench_served(args, dev, rank, world, local)
     if rank == 0:
-        out = {"metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": value / PUBLISHED_SUBSTEPS_PER_S, "dtype": "f32",
-               "data": "synthetic (seeded ellipsoid particles, reference heater geometry)",
-               "config": {"workload": WORKLOAD, "n": n, "cells": N, "spinup": args.spinup, "parallelism": f"replicas x{world}",
-                          "l2": "scene state ~170 MB > 126 MB L2 (inputs larger than L2); the CG working set "
-                                "(~35 MB) stays L2-resident within a substep by design",
-                          "mean_pressure_iters": p_iters / args.steps, "mean_heat_iters": h_iters / args.steps,
-                          "cell_updates_per_s": value * N, "substep_status": int(st1.status)},
-               "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
-               "clocks": ck}
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -211,20 +211,10 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
     int grid = p->persistent_blocks > 0 ? p->persistent_blocks : d->sms * per_sm;
     if (grid > d->sms * occ) grid = d->sms * occ;
     if (grid > p->num_tiles) grid = p->num_tiles;
-    // every block keeps the scalars of the scenes its contiguous tile range touches (at most 32)
-    std::vector<int> begin(p->num_scenes + 1, 0);
-    for (int s = 0; s < p->num_scenes; ++s) {
-        const hf_scene& sc = p->scenes_host[s];
-        begin[s + 1] = begin[s] + ((sc.flags & HF_FLAG_ACTIVE) ? tiles_of(sc.n) : 0);
-    }
-    if (begin[p->num_scenes] != p->num_tiles) return fail(HF_ERR_ARG, "plan changed since hf_plan_upload");
-    for (int b = 0; b < grid; ++b) {
-        const int c0 = (int)(((long long)p->num_tiles * b) / grid), c1 = (int)(((long long)p->num_tiles * (b + 1)) / grid);
-        if (c1 <= c0) continue;
-        const int s0 = (int)(std::upper_bound(begin.begin(), begin.end(), c0) - begin.begin()) - 1;
-        const int s1 = (int)(std::upper_bound(begin.begin(), begin.end(), c1 - 1) - begin.begin()) - 1;
-        if (s1 - s0 + 1 > 32) return fail(HF_ERR_ARG, "more than 32 scenes in one block's tile range: use more blocks");
-    }
+    int total = 0;
+    for (int s = 0; s < p->num_scenes; ++s)
+        if (p->scenes_host[s].flags & HF_FLAG_ACTIVE) total += tiles_of(p->scenes_host[s].n);
+    if (total != p->num_tiles) return fail(HF_ERR_ARG, "plan changed since hf_plan_upload");
     void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&nt, (void*)&ns, (void*)&dt, (void*)&ws};
     HF_CUDA(cudaLaunchCooperativeKernel(hf::pcg_kernel(heat), dim3(grid), dim3(hf::kThreads), args, 0, S(stream)),
             "cooperative launch (CG)");

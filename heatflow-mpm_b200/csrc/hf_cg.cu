@@ -33,7 +33,6 @@
 namespace hf {
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;   // 2 s
-constexpr int kLocalScenes = 32;                                  // scenes one streaming block may touch
 
 __device__ __forceinline__ int uidx_(int n, int i, int j, int k) { return (i * n + j) * n + k; }
 __device__ __forceinline__ int vidx_(int n, int i, int j, int k) { return (i * (n + 1) + j) * n + k; }
@@ -318,46 +317,82 @@ __device__ __forceinline__ void write_stats(const hf_scene& S, const LocalScene&
 }
 
 // ================================================================================================== streaming
+// Scene scalars live in the scene's control record; only the scene's owner block (scene s -> block s % gridDim.x)
+// writes it, in the reduction steps between phases, and every block reads it after the next grid barrier.
+__device__ __forceinline__ LocalScene ctl_load(const CgCtl* c) {
+    LocalScene L;
+    L.bb = __ldcg(&c->bb);
+    L.rr = __ldcg(&c->rr);
+    L.rz = __ldcg(&c->rz);
+    L.pAp = __ldcg(&c->pAp);
+    L.atol_sq = __ldcg(&c->atol_sq);
+    L.mean = __ldcg(&c->mean);
+    L.alpha = __ldcg(&c->alpha);
+    L.beta = __ldcg(&c->beta);
+    L.iters = __ldcg(&c->iters);
+    L.live = __ldcg(&c->live);
+    L.status = __ldcg(&c->status);
+    L.maxit = __ldcg(&c->maxit);
+    return L;
+}
+
+__device__ __forceinline__ void ctl_store(CgCtl* c, const LocalScene& L) {
+    c->bb = L.bb;
+    c->rr = L.rr;
+    c->rz = L.rz;
+    c->pAp = L.pAp;
+    c->atol_sq = L.atol_sq;
+    c->mean = L.mean;
+    c->alpha = L.alpha;
+    c->beta = L.beta;
+    c->iters = L.iters;
+    c->live = L.live;
+    c->status = L.status;
+    c->maxit = L.maxit;
+}
+
+// Tiles are dealt round-robin (tile c to block c % gridDim.x), so every block holds an equal share of every live
+// scene and stays busy while scenes converge at different iterations.  Per iteration:
+//   phase A (tiles of live scenes) | barrier | owners: pAp -> alpha | barrier |
+//   phase B (tiles of live scenes) | barrier | owners: r.r, r.z -> beta, convergence | barrier
 template <bool HEAT>
 __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles,
                                                  int num_tiles, int num_scenes, double dt_d, Workspace ws) {
     __shared__ double red[6 * 32];
     __shared__ unsigned char s_par[kMaxScenes];
-    __shared__ LocalScene loc[kLocalScenes];
+    __shared__ unsigned char s_live[kMaxScenes];
+    __shared__ float s_coef[kMaxScenes];   // beta in phase A, alpha in phase B
     for (int s = threadIdx.x; s < num_scenes; s += kThreads) s_par[s] = (unsigned char)scenes[s].state->parity;
-    const int c0 = (int)(((long long)num_tiles * blockIdx.x) / gridDim.x);
-    const int c1 = (int)(((long long)num_tiles * (blockIdx.x + 1)) / gridDim.x);
-    const int s_lo = c0 < c1 ? tiles[c0].scene : 0;
-    const int s_hi = c0 < c1 ? tiles[c1 - 1].scene : -1;
-    __syncthreads();
     unsigned* bar = ws.bar + (HEAT ? 0 : 1);
     unsigned* live_count = ws.live_count + (HEAT ? 0 : 1);
     double* bufA = ws.partA;
     double* bufB = ws.partB;
+    CgCtl* ctl = ws.ctl;
     unsigned epoch = 0;
     const float dt = (float)dt_d;
     const int lt = threadIdx.x;
+    const int G = gridDim.x;
+    __syncthreads();
 
     // ---------------------------------------------------------------------------------------- prologue
-    for (int s = s_lo; s <= s_hi; ++s) {
-        if (!HEAT) {
+    if (!HEAT) {
+        // the pressure rhs mean of every scene (grid.py:238-241), summed by the scene's owner
+        for (int s = blockIdx.x; s < num_scenes; s += G) {
             double m[1];
             const int comp[1] = {0};
             scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[s], ws.chunk_begin[s + 1], comp, m, red);
             const int n = scenes[s].n;
-            if (threadIdx.x == 0) loc[s - s_lo].mean = (double)__double2float_rn(m[0] / ((double)n * n * n));
-        } else if (threadIdx.x == 0) {
-            loc[s - s_lo].mean = 0.0;
+            if (threadIdx.x == 0) ctl[s].mean = (double)__double2float_rn(m[0] / ((double)n * n * n));
         }
+        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
     }
-    __syncthreads();
-    for (int c = c0; c < c1; ++c) {
+    for (int c = blockIdx.x; c < num_tiles; c += G) {
         const TileItem ti = tiles[c];
         const hf_scene& S = scenes[ti.scene];
         const int n = S.n, par = s_par[ti.scene];
         const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
         const float* x = HEAT ? S.T[par ^ 1] : S.p;
-        const float mean = (float)loc[ti.scene - s_lo].mean;
+        const float mean = HEAT ? 0.0f : (float)__ldcg(&ctl[ti.scene].mean);
         double part[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
@@ -381,53 +416,39 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
         }
     }
     if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+    for (int s = blockIdx.x; s < num_scenes; s += G) {
+        const int b = ws.tile_begin[s], e = ws.tile_begin[s + 1];
+        double tot[3];
+        const int comp[3] = {0, 1, 2};
+        scene_sums<3>(bufB, b, e, comp, tot, red);
+        if (threadIdx.x == 0) {
+            const hf_scene& S = scenes[s];
+            LocalScene L;
+            init_scalars(L, S, HEAT, tot, S.n * S.n * S.n);
+            L.mean = HEAT ? 0.0 : __ldcg(&ctl[s].mean);
+            L.live = L.live && b < e;
+            L.pAp = 0.0;
+            ctl_store(&ctl[s], L);
+            if (L.live) atomicAdd(live_count, 1u);
+        }
+    }
+    if (!grid_barrier(bar, epoch, ws.err)) goto finish;
 
     // ------------------------------------------------------------------------------------------ iterations
-    for (int kit = 1;; ++kit) {
-        for (int s = s_lo; s <= s_hi; ++s) {
-            LocalScene& L = loc[s - s_lo];
-            const hf_scene& S = scenes[s];
-            const int b = ws.tile_begin[s], e = ws.tile_begin[s + 1];
-            const bool owner = b >= c0 && b < c1;
-            if (kit == 1) {
-                double tot[3];
-                const int comp[3] = {0, 1, 2};
-                scene_sums<3>(bufB, b, e, comp, tot, red);
-                if (threadIdx.x == 0) {
-                    const double mean = L.mean;
-                    init_scalars(L, S, HEAT, tot, S.n * S.n * S.n);
-                    L.mean = mean;
-                    L.live = L.live && b < e;
-                    if (owner && L.live) atomicAdd(live_count, 1u);
-                }
-            } else {
-                if (!L.live) continue;   // uniform: shared value read after the last __syncthreads
-                double tot[2];
-                const int comp[2] = {1, 2};
-                scene_sums<2>(bufB, b, e, comp, tot, red);
-                if (threadIdx.x == 0 && !update_scalars(L, HEAT, tot[0], tot[1], kit - 1) && owner) atomicSub(live_count, 1u);
-            }
-            __syncthreads();
-            if (owner && threadIdx.x == 0 && !L.live) {
-                CgCtl& W = ws.ctl[s];
-                W.bb = L.bb;
-                W.rr = L.rr;
-                W.atol_sq = L.atol_sq;
-                W.iters = L.iters;
-                W.status = L.status;
-                W.mean = L.mean;
-            }
-            __syncthreads();
+    for (int kit = 1; *(volatile unsigned*)live_count != 0u; ++kit) {
+        for (int s = threadIdx.x; s < num_scenes; s += kThreads) {
+            s_live[s] = (unsigned char)(__ldcg(&ctl[s].live) != 0);
+            s_coef[s] = __ldcg(&ctl[s].beta);
         }
+        __syncthreads();
         // phase A: p_k at the stencil points, Ap = A p_k, p.Ap
-        for (int c = c0; c < c1; ++c) {
+        for (int c = blockIdx.x; c < num_tiles; c += G) {
             const TileItem ti = tiles[c];
-            const LocalScene& L = loc[ti.scene - s_lo];
-            if (!L.live) continue;
+            if (!s_live[ti.scene]) continue;
             const hf_scene& S = scenes[ti.scene];
             const int n = S.n;
             const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
-            const Dir P{S.cg_z, S.cg_p[(kit - 1) & 1], L.beta, kit == 1};
+            const Dir P{S.cg_z, S.cg_p[(kit - 1) & 1], s_coef[ti.scene], kit == 1};
             float pc[4], ap[4];
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
@@ -457,30 +478,29 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
             if (lt == 0) bufA[3 * c] = part[0];
         }
         if (!grid_barrier(bar, epoch, ws.err)) goto finish;
-        if (*(volatile unsigned*)live_count == 0u) break;
-        for (int s = s_lo; s <= s_hi; ++s) {
-            LocalScene& L = loc[s - s_lo];
-            if (!L.live) continue;
+        for (int s = blockIdx.x; s < num_scenes; s += G) {
+            if (!s_live[s]) continue;
             double tot[1];
             const int comp[1] = {0};
             scene_sums<1>(bufA, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
             if (threadIdx.x == 0) {
-                L.pAp = tot[0];
-                L.alpha = __double2float_rn(L.rz / tot[0]);
+                ctl[s].pAp = tot[0];
+                ctl[s].alpha = __double2float_rn(__ldcg(&ctl[s].rz) / tot[0]);
             }
-            __syncthreads();
         }
+        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        for (int s = threadIdx.x; s < num_scenes; s += kThreads) s_coef[s] = __ldcg(&ctl[s].alpha);
+        __syncthreads();
         // phase B: x += alpha p, r -= alpha Ap, z = D r, r.r and r.z
-        for (int c = c0; c < c1; ++c) {
+        for (int c = blockIdx.x; c < num_tiles; c += G) {
             const TileItem ti = tiles[c];
-            const LocalScene& L = loc[ti.scene - s_lo];
-            if (!L.live) continue;
+            if (!s_live[ti.scene]) continue;
             const hf_scene& S = scenes[ti.scene];
             const int n = S.n, par = s_par[ti.scene];
             float* x = HEAT ? S.T[par ^ 1] : S.p;
             const float* D = HEAT ? S.hdiag : S.pdiag;
             const float* pk = S.cg_p[kit & 1];
-            const float alpha = L.alpha;
+            const float alpha = s_coef[ti.scene];
             float xv[4], rv[4], zv[4];
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
@@ -509,10 +529,22 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
             }
         }
         if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        for (int s = blockIdx.x; s < num_scenes; s += G) {
+            if (!s_live[s]) continue;
+            double tot[2];
+            const int comp[2] = {1, 2};
+            scene_sums<2>(bufB, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
+            if (threadIdx.x == 0) {
+                LocalScene L = ctl_load(&ctl[s]);
+                if (!update_scalars(L, HEAT, tot[0], tot[1], kit)) atomicSub(live_count, 1u);
+                ctl_store(&ctl[s], L);
+            }
+        }
+        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
     }
     // -------------------------------------------------------------------- pressure epilogue: projection
     if (!HEAT) {
-        for (int c = c0; c < c1; ++c) {
+        for (int c = blockIdx.x; c < num_tiles; c += G) {
             const TileItem ti = tiles[c];
             const hf_scene& S = scenes[ti.scene];
             const int n = S.n, par = s_par[ti.scene];
@@ -525,22 +557,14 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
         }
     }
 finish:
-    // Owners recorded their scene before the last barrier; every block read the parities before its first barrier,
-    // so block 0 may flip them now.
+    // Every block read the parities before its first barrier, so block 0 may flip them now; the control records were
+    // final at the last barrier.
     if (blockIdx.x == 0) {
         const bool timed_out = *(volatile int*)ws.err != 0;
         for (int s = threadIdx.x; s < num_scenes; s += kThreads) {
             const hf_scene& S = scenes[s];
             if (!(S.flags & HF_FLAG_ACTIVE)) continue;
-            const CgCtl& C = ws.ctl[s];
-            LocalScene L;
-            L.bb = C.bb;
-            L.rr = C.rr;
-            L.atol_sq = C.atol_sq;
-            L.iters = C.iters;
-            L.status = C.status;
-            L.mean = C.mean;
-            write_stats(S, L, HEAT, timed_out, s_par[s]);
+            write_stats(S, ctl_load(&ctl[s]), HEAT, timed_out, s_par[s]);
         }
     }
 }

@@ -17,27 +17,36 @@ CP_AIR = 1005.0   # heat capacity of air [J/(kg K)] (heater.py:7)
 AIR, SHELL, ROD, FAN, TROUGH = 0, 1, 2, 3, 4
 
 
-def face_weights(solid: np.ndarray, fan: np.ndarray, fan_speed: float, facing) -> tuple[list, list]:
-    """Static relaxation weights of the three face lattices (heater.py:54-63).
-
-    A face touching a solid cell gets K_SOLID; otherwise a face touching a fan cell gets K_FAN, and its
-    momentum weight K_FAN * fan_speed * facing[axis].  Domain faces see the outside as empty."""
-    k_faces, m_faces = [], []
+def face_masks(solid: np.ndarray, fan: np.ndarray) -> tuple[list, list]:
+    """Per face lattice: does the face touch a solid cell, and does it touch a fan cell but no solid one
+    (heater.py:54-63; domain faces see the outside as empty)."""
+    touch_solid, touch_fan = [], []
     for axis in range(3):
         widths = [(0, 0), (0, 0), (0, 0)]
         widths[axis] = (1, 1)
         sp, fp = np.pad(solid, widths), np.pad(fan, widths)
         n_faces = solid.shape[axis] + 1
-        below = np.take(sp, np.arange(0, n_faces), axis=axis)
-        above = np.take(sp, np.arange(1, n_faces + 1), axis=axis)
-        touches_solid = below | above
-        touches_fan = (np.take(fp, np.arange(0, n_faces), axis=axis) | np.take(fp, np.arange(1, n_faces + 1), axis=axis)) \
-            & ~touches_solid
-        k = np.where(touches_solid, K_SOLID, np.where(touches_fan, K_FAN, 0.0)).astype(np.float32)
-        m = np.where(touches_fan, K_FAN * fan_speed * facing[axis], 0.0).astype(np.float32)
-        k_faces.append(k)
-        m_faces.append(m)
-    return k_faces, m_faces
+        lo, hi = np.arange(0, n_faces), np.arange(1, n_faces + 1)
+        ts = np.take(sp, lo, axis=axis) | np.take(sp, hi, axis=axis)
+        touch_solid.append(ts)
+        touch_fan.append((np.take(fp, lo, axis=axis) | np.take(fp, hi, axis=axis)) & ~ts)
+    return touch_solid, touch_fan
+
+
+def fan_momentum(touch_fan: list, fan_speed: float, facing) -> list:
+    """Momentum weights K_FAN * fan_speed * facing[axis] on the fan faces of face_masks (heater.py:61-62)."""
+    return [np.where(touch_fan[axis], K_FAN * fan_speed * facing[axis], 0.0).astype(np.float32) for axis in range(3)]
+
+
+def face_weights(solid: np.ndarray, fan: np.ndarray, fan_speed: float, facing) -> tuple[list, list]:
+    """Static relaxation weights of the three face lattices (heater.py:54-63).
+
+    A face touching a solid cell gets K_SOLID; otherwise a face touching a fan cell gets K_FAN, and its
+    momentum weight K_FAN * fan_speed * facing[axis]."""
+    touch_solid, touch_fan = face_masks(solid, fan)
+    k_faces = [np.where(ts, K_SOLID, np.where(tf, K_FAN, 0.0)).astype(np.float32)
+               for ts, tf in zip(touch_solid, touch_fan)]
+    return k_faces, fan_momentum(touch_fan, fan_speed, facing)
 
 
 def source_rate(power: float, rho_air: float, n_source: int, h: float) -> float:
@@ -108,9 +117,11 @@ class Heater:
 
 @dataclass
 class BoxHeater:
-    """Box heater of the synthetic air-only plume scene: a block of rod cells on the floor with a layer of heated
-    air on top.  Block cells i in [round(x/h) - bx//2, +bx), j in [n//2 - by//2, +by), k in [0, bz) are rods
-    (solid, fixed at t_rod); the bx x by layer at k = bz is trough air (the power source).  Same interface as Heater."""
+    """Box heater of the synthetic air-only scenes: a block of rod cells on the floor with a layer of heated air on
+    top.  Block cells i in [round(x/h) - bx//2, +bx), j in [n//2 - by//2, +by), k in [0, bz) are rods (solid, fixed at
+    t_rod); the bx x by layer at k = bz is trough air (the power source); with fan > 0 the layer above it is a fan
+    outlet blowing upward (class 3, relaxation weight K_FAN toward fan m/s, as heater.py:54-63 does for the trough
+    heater).  Same interface as Heater."""
     x: float = 0.10
     block: tuple = (4, 4, 2)
     t_rod: float = 300.0
@@ -127,11 +138,13 @@ class BoxHeater:
         if self.on:
             cells[i0:i0 + bx, j0:j0 + by, 0:bz] = ROD
             cells[i0:i0 + bx, j0:j0 + by, bz] = TROUGH
+            if self.fan > 0:
+                cells[i0:i0 + bx, j0:j0 + by, bz + 1] = FAN
         solid = cells == ROD
-        source = cells == TROUGH
+        source = (cells == TROUGH) | (cells == FAN)
         rate = source_rate(self.power, rho_air, int(source.sum()), h) if self.on else 0.0
         facing = (0.0, 0.0, 1.0)
-        k_faces, m_faces = face_weights(solid, np.zeros_like(solid), self.fan, facing)
+        k_faces, m_faces = face_weights(solid, cells == FAN, self.fan, facing)
         c = [(i0 + bx / 2) * h, (j0 + by / 2) * h, bz * h / 2]
         geom = dict(centre=c, facing=list(facing), axis=[1.0, 0.0, 0.0], up=[0.0, 0.0, 1.0])
         return cells, solid, source, rate, k_faces, m_faces, geom

@@ -87,9 +87,10 @@ class DeviceScene:
         coupled = spec.n_particles > 0
         has_static = spec.static_alpha is not None
         if has_static:
-            self.st_alpha = torch.as_tensor(np.ascontiguousarray(spec.static_alpha, np.float32), device=dev)
-            self.st_k = [torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev) for a in spec.static_k]
-            self.st_m = [torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev) for a in spec.static_m]
+            up = lambda a: torch.as_tensor(np.require(a, np.float32, ("C", "W")), device=dev)   # host copy if read-only
+            self.st_alpha = up(spec.static_alpha)
+            self.st_k = [up(a) for a in spec.static_k]
+            self.st_m = [up(a) for a in spec.static_m]
         else:
             self.st_alpha, self.st_k, self.st_m = None, [None] * 3, [None] * 3
         if coupled:
@@ -134,7 +135,7 @@ class DeviceScene:
     def _set_flags(self, fixed, tfix, source):
         flags = np.asarray(fixed, bool).astype(np.uint8) | (np.asarray(source, bool).astype(np.uint8) << 1)
         self.cell_flags.copy_(torch.as_tensor(flags, device=self.device))
-        self.tfix.copy_(torch.as_tensor(np.ascontiguousarray(tfix, np.float32), device=self.device))
+        self.tfix.copy_(torch.as_tensor(np.require(tfix, np.float32, ("C", "W")), device=self.device))
 
     def set_fixed(self, fixed, values):
         """heat.py:189-192: new Dirichlet mask and values, applied to T at once."""

@@ -130,16 +130,16 @@ class OracleScene:
         for i, ax in enumerate("xyz"):
             for pre in ("a", "q", "k", "m"):
                 self.a[pre + ax] = z(fs[i])
-            self.a["st_k" + ax] = z(fs[i]) if static_k is None else np.ascontiguousarray(static_k[i], dt)
-            self.a["st_m" + ax] = z(fs[i]) if static_m is None else np.ascontiguousarray(static_m[i], dt)
+            self.a["st_k" + ax] = z(fs[i]) if static_k is None else np.array(static_k[i], dt, order="C")
+            self.a["st_m" + ax] = z(fs[i]) if static_m is None else np.array(static_m[i], dt, order="C")
         for nm in self.FIELDS_CELL:
             self.a[nm] = z(N)
         if static_alpha is not None:
-            self.a["st_alpha"] = np.ascontiguousarray(static_alpha, dt)
+            self.a["st_alpha"] = np.array(static_alpha, dt, order="C")
         self.a["fixed"] = np.zeros(N, np.int32) if fixed is None else np.ascontiguousarray(fixed, np.int32)
         self.a["src"] = np.zeros(N, np.int32) if src is None else np.ascontiguousarray(src, np.int32)
         if tfix is not None:
-            self.a["tfix"] = np.ascontiguousarray(tfix, dt)
+            self.a["tfix"] = np.array(tfix, dt, order="C")
         for nm in ("T", "T2", "Tw"):
             self.a[nm][...] = t_amb if t_init_grid is None else t_init_grid
         P = 0 if particles is None else len(particles)
