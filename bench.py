@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="plain line without the batched/served summaries")
     ap.add_argument("--scenes", type=int, default=64, help="batched: scenes in the ensemble")
     ap.add_argument("--graph-steps", type=int, default=10, help="batched: substeps per captured CUDA graph")
+    ap.add_argument("--edges", default="32,48,64,96,128", help="batched: grid edges the ensemble draws from")
+    ap.add_argument("--no-autotune", action="store_true", help="batched: default launch shape, no tuning")
+    ap.add_argument("--launch", default=None, help="batched: fixed CG launch shape 'blocks,group_cells,lanes'")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="served: length of the trace window")
     ap.add_argument("--rate", type=float, default=20.0, help="served: mean arrivals per second")
     ap.add_argument("--hbm-budget", type=float, default=150e9, help="served: HBM admitted for scenes, bytes")
@@ -371,12 +374,19 @@ def bench_plain(args, dev, rank, world, local):
 def bench_batched(args, dev, rank, world, local, steps, warmup, cpu_sample=True):
     import torch
     from heatflow_mpm.batch import AirBatch, autotune, ensemble, shard_scenarios
-    scs_all = ensemble(count=args.scenes, seed=0, steps=steps)
+    scs_all = ensemble(count=args.scenes, seed=0, edges=tuple(int(e) for e in args.edges.split(",")), steps=steps)
     mine = shard_scenarios(scs_all, rank, world)
     t_build = time.perf_counter()
     batch = AirBatch(mine, device=dev)
     t_build = time.perf_counter() - t_build
-    pb, tune = autotune(batch, dt=DT, reps=2)
+    if args.launch:
+        pb, gc, lanes = (int(v) for v in args.launch.split(","))
+        batch.plan.plan.persistent_blocks, batch.plan.plan.group_cells, batch.plan.lanes = pb, gc, lanes
+        tune = None
+    elif args.no_autotune:
+        (pb, gc, lanes), tune = (0, 0, 0), None
+    else:
+        (pb, gc, lanes), tune = autotune(batch, dt=DT, reps=2)
     for _ in range(warmup):
         batch.substep(DT)
     G = max(1, min(args.graph_steps, steps))
@@ -463,6 +473,7 @@ def bench_batched(args, dev, rank, world, local, steps, warmup, cpu_sample=True)
                                    f"h=0.48 m/edge, box heater x U(0.05,0.2) m, 100-800 W, fan 0-3 m/s, dt=2 ms, "
                                    f"pressure tol 1e-4, heat tol 1e-6",
                        "scenes": args.scenes, "cells": int(cells), "graph_substeps": G, "persistent_blocks": pb,
+                       "group_cells": gc, "lanes": lanes,
                        "autotune_ms": tune, "parallelism": f"scene-sharded x{world}",
                        "l2": f"{cells * 4 * 40 / 1e9:.1f} GB of scene state > 126 MB L2 (inputs larger than L2)",
                        "scene_substeps_per_s": len(scs_all) * steps / (el_ms / 1000.0),

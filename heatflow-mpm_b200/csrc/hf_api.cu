@@ -71,6 +71,9 @@ int device_info(DeviceInfo** out) {
     return HF_OK;
 }
 
+constexpr long long kGroupCells = 2400000;   // cells of one CG group by default (one 128^3 or two 96^3 scenes)
+constexpr size_t kHeadBytes = 256;           // barrier counters, group queue, lane slots, timeout flag
+
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
@@ -80,8 +83,8 @@ struct Layout {
 Layout layout(int S, int C, int T) {
     Layout L{};
     size_t o = 0;
-    L.head = o;                      // bar[2], live_count[2], err, pad -> 64 bytes
-    o = align_up(o + 64, 256);
+    L.head = o;                      // bar[2 kMaxLanes], queue[2], lane_next[2 kMaxLanes], err -> 256 bytes
+    o = align_up(o + kHeadBytes, 256);
     L.chunk_begin = o;
     o = align_up(o + sizeof(int) * (size_t)(S + 1), 256);
     L.tile_begin = o;
@@ -103,8 +106,9 @@ hf::Workspace workspace(const hf_plan* p) {
     char* b = static_cast<char*>(p->workspace);
     hf::Workspace w;
     w.bar = reinterpret_cast<unsigned*>(b + L.head);
-    w.live_count = w.bar + 2;
-    w.err = reinterpret_cast<int*>(w.bar + 4);
+    w.queue = w.bar + 2 * hf::kMaxLanes;
+    w.lane_next = reinterpret_cast<int*>(w.queue + 2);
+    w.err = w.lane_next + 2 * hf::kMaxLanes;
     w.chunk_begin = reinterpret_cast<int*>(b + L.chunk_begin);
     w.tile_begin = reinterpret_cast<int*>(b + L.tile_begin);
     w.ctl = reinterpret_cast<hf::CgCtl*>(b + L.ctl);
@@ -154,68 +158,110 @@ bool any_flag(const hf_plan* p, unsigned f) {
     return false;
 }
 
+// The resident variant for a plan with one active scene whose tiles fit one block per SM.  Returns HF_OK after
+// launching, or -1 when the scene does not fit (the caller falls back to the streaming kernel).
+int launch_resident(const hf_plan* p, const DeviceInfo* d, bool heat, double dt, int s, void* stream) {
+    hf::Workspace ws = workspace(p);
+    const hf_scene* scenes = static_cast<const hf_scene*>(p->scenes_dev);
+    const hf::TileItem* tiles = static_cast<const hf::TileItem*>(p->tiles_dev);
+    const hf_scene& sc = p->scenes_host[s];
+    int t_lo = 0, t_hi = p->num_tiles, rc;
+    const int nt = t_hi - t_lo;
+    const int G = nt < d->sms ? nt : d->sms;
+    const int tpb = (nt + G - 1) / G;
+    const bool tma = !heat && (sc.n % 4 == 0) && !(p->options & HF_PLAN_NO_TMA);
+    for (int m = 1; m <= 3; ++m) {
+        const int groups = (tpb + m - 1) / m;
+        if (groups > kResGroupsMax[m]) continue;
+        const void* fn = hf::pcg_resident_kernel(heat, m, tma);
+        const size_t smem = hf::pcg_resident_smem(groups, m, tma);
+        if (smem > d->smem_optin) continue;
+        if (smem > 48 * 1024)
+            HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+        int occ = 0;
+        HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256 * groups, smem), "occupancy (resident)");
+        if (occ < 1) continue;
+        hf::TileMaps maps;
+        std::memset(&maps, 0, sizeof maps);
+        if (tma) {
+            const int n = sc.n;
+            if ((rc = encode_map(&maps.z, sc.cg_z, n, n, n, 40, 10, 6))) return rc;
+            if ((rc = encode_map(&maps.p0, sc.cg_p[0], n, n, n, 40, 10, 6))) return rc;
+            if ((rc = encode_map(&maps.p1, sc.cg_p[1], n, n, n, 40, 10, 6))) return rc;
+            if ((rc = encode_map(&maps.ax, sc.ax, n, n, n + 1, 32, 8, 5))) return rc;
+            if ((rc = encode_map(&maps.ayc, sc.ayc, n, n, n, 32, 9, 4))) return rc;
+            if ((rc = encode_map(&maps.azc, sc.azc, n, n, n, 36, 8, 4))) return rc;
+        }
+        HF_CUDA(cudaMemsetAsync(ws.bar, 0, kHeadBytes, S(stream)), "cudaMemsetAsync(barrier)");
+        void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&t_lo, (void*)&t_hi, (void*)&dt, (void*)&ws, (void*)&maps};
+        HF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(256 * groups), args, smem, S(stream)),
+                "cooperative launch (resident CG)");
+        return HF_OK;
+    }
+    return -1;
+}
+
+// Both CG solves of a plan.  One active scene: the resident variant where it fits.  Otherwise one launch of the
+// streaming kernel: the active scenes are cut, in table order, into groups of at most kGroupScenes scenes and
+// group_cells cells (default kGroupCells: a group's CG vectors stay in L2), solved by the lanes of the grid.
 int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
     DeviceInfo* d = nullptr;
     int rc = device_info(&d);
     if (rc) return rc;
     if (p->num_tiles == 0) return HF_OK;
-    hf::Workspace ws = workspace(p);
-    const hf_scene* scenes = static_cast<const hf_scene*>(p->scenes_dev);
-    const hf::TileItem* tiles = static_cast<const hf::TileItem*>(p->tiles_dev);
-    int nt = p->num_tiles, ns = p->num_scenes;
-    // barrier counters, live counts and the timeout flag start at zero for every solve
-    HF_CUDA(cudaMemsetAsync(ws.bar, 0, 64, S(stream)), "cudaMemsetAsync(barrier)");
-    // register-resident variant: one active scene whose tiles fit one block per SM
-    int active = -1, nactive = 0;
+    int nactive = 0, last = -1, total = 0;
     for (int s = 0; s < p->num_scenes; ++s)
         if (p->scenes_host[s].flags & HF_FLAG_ACTIVE) {
-            active = s;
             ++nactive;
+            last = s;
+            total += tiles_of(p->scenes_host[s].n);
         }
+    if (total != p->num_tiles) return fail(HF_ERR_ARG, "plan changed since hf_plan_upload");
     if (nactive == 1 && !(p->options & HF_PLAN_STREAMING_CG)) {
-        const hf_scene& sc = p->scenes_host[active];
-        const int G = p->num_tiles < d->sms ? p->num_tiles : d->sms;
-        const int tpb = (p->num_tiles + G - 1) / G;
-        const bool tma = !heat && (sc.n % 4 == 0) && !(p->options & HF_PLAN_NO_TMA);
-        for (int m = 1; m <= 3; ++m) {
-            const int groups = (tpb + m - 1) / m;
-            if (groups > kResGroupsMax[m]) continue;
-            const void* fn = hf::pcg_resident_kernel(heat, m, tma);
-            const size_t smem = hf::pcg_resident_smem(groups, m, tma);
-            if (smem > d->smem_optin) continue;
-            if (smem > 48 * 1024)
-                HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
-            int occ = 0;
-            HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256 * groups, smem), "occupancy (resident)");
-            if (occ < 1) continue;
-            hf::TileMaps maps;
-            std::memset(&maps, 0, sizeof maps);
-            if (tma) {
-                const int n = sc.n;
-                if ((rc = encode_map(&maps.z, sc.cg_z, n, n, n, 40, 10, 6))) return rc;
-                if ((rc = encode_map(&maps.p0, sc.cg_p[0], n, n, n, 40, 10, 6))) return rc;
-                if ((rc = encode_map(&maps.p1, sc.cg_p[1], n, n, n, 40, 10, 6))) return rc;
-                if ((rc = encode_map(&maps.ax, sc.ax, n, n, n + 1, 32, 8, 5))) return rc;
-                if ((rc = encode_map(&maps.ayc, sc.ayc, n, n, n, 32, 9, 4))) return rc;
-                if ((rc = encode_map(&maps.azc, sc.azc, n, n, n, 36, 8, 4))) return rc;
-            }
-            void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&nt, (void*)&ns, (void*)&dt, (void*)&ws, (void*)&maps};
-            HF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(256 * groups), args, smem, S(stream)),
-                    "cooperative launch (resident CG)");
-            return HF_OK;
+        rc = launch_resident(p, d, heat, dt, last, stream);
+        if (rc != -1) return rc;
+    }
+    static thread_local hf::GroupTable gt;   // 16 KB: kept off the stack; the launch copies it
+    gt.count = 0;
+    const long long budget = p->group_cells > 0 ? p->group_cells : kGroupCells;
+    int s_lo = -1, s_last = -1, t_lo = 0, t = 0;
+    long long cells = 0;
+    for (int s = 0; s <= p->num_scenes; ++s) {
+        const bool end = s == p->num_scenes;
+        if (!end && !(p->scenes_host[s].flags & HF_FLAG_ACTIVE)) continue;
+        const long long c = end ? 0 : (long long)p->scenes_host[s].n * p->scenes_host[s].n * p->scenes_host[s].n;
+        if (s_lo >= 0 && (end || cells + c > budget || s + 1 - s_lo > hf::kGroupScenes)) {
+            // the group ends after its last active scene: [s_lo, s_last] spans at most kGroupScenes scenes
+            if (gt.count == hf::kMaxGroups) return fail(HF_ERR_ARG, "more CG groups than one launch takes");
+            gt.g[gt.count++] = make_int4(s_lo, s_last + 1, t_lo, t);
+            s_lo = -1;
         }
+        if (end) break;
+        if (s_lo < 0) {
+            s_lo = s;
+            t_lo = t;
+            cells = 0;
+        }
+        cells += c;
+        s_last = s;
+        t += tiles_of(p->scenes_host[s].n);
     }
     const int occ = heat ? d->occ_heat : d->occ_pressure;
     if (occ <= 0) return fail(HF_ERR_DEVICE, "persistent CG kernel does not fit on an SM");
-    int per_sm = occ < 2 ? occ : 2;
-    int grid = p->persistent_blocks > 0 ? p->persistent_blocks : d->sms * per_sm;
+    int lanes = (int)((p->options >> HF_PLAN_LANES_SHIFT) & 15u);
+    if (lanes <= 0) lanes = 1;
+    if (lanes > hf::kMaxLanes) lanes = hf::kMaxLanes;
+    if (lanes > gt.count) lanes = gt.count;
+    int grid = p->persistent_blocks > 0 ? p->persistent_blocks : d->sms * (occ < 2 ? occ : 2);
     if (grid > d->sms * occ) grid = d->sms * occ;
-    if (grid > p->num_tiles) grid = p->num_tiles;
-    int total = 0;
-    for (int s = 0; s < p->num_scenes; ++s)
-        if (p->scenes_host[s].flags & HF_FLAG_ACTIVE) total += tiles_of(p->scenes_host[s].n);
-    if (total != p->num_tiles) return fail(HF_ERR_ARG, "plan changed since hf_plan_upload");
-    void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&nt, (void*)&ns, (void*)&dt, (void*)&ws};
+    grid -= grid % lanes;
+    if (grid < lanes) grid = lanes;
+    gt.lanes = lanes;
+    hf::Workspace ws = workspace(p);
+    const hf_scene* scenes = static_cast<const hf_scene*>(p->scenes_dev);
+    const hf::TileItem* tiles = static_cast<const hf::TileItem*>(p->tiles_dev);
+    HF_CUDA(cudaMemsetAsync(ws.bar, 0, kHeadBytes, S(stream)), "cudaMemsetAsync(barrier)");
+    void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&dt, (void*)&ws, (void*)&gt};
     HF_CUDA(cudaLaunchCooperativeKernel(hf::pcg_kernel(heat), dim3(grid), dim3(hf::kThreads), args, 0, S(stream)),
             "cooperative launch (CG)");
     return HF_OK;

@@ -38,14 +38,14 @@ __device__ __forceinline__ int uidx_(int n, int i, int j, int k) { return (i * n
 __device__ __forceinline__ int vidx_(int n, int i, int j, int k) { return (i * (n + 1) + j) * n + k; }
 __device__ __forceinline__ int widx_(int n, int i, int j, int k) { return (i * n + j) * (n + 1) + k; }
 
-// Grid barrier with a bounded wait.  Thread 0 publishes the block's writes with a release reduction (cumulative over
+// Barrier of nblocks blocks (the grid, or one lane of it) with a bounded wait.  Thread 0 publishes the block's writes with a release reduction (cumulative over
 // the writes the block's threads made before __syncthreads) and polls with acquire loads.  Returns false (in every
 // thread) once any block has timed out.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* err) {
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* err, unsigned nblocks) {
     ++epoch;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned target = epoch * gridDim.x;
+        const unsigned target = epoch * nblocks;
         asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
         const unsigned long long t0 = global_timer_ns();
         unsigned spins = 0;
@@ -188,6 +188,57 @@ __device__ __forceinline__ float heat_nt(const hf_scene& S, const X& x, float xc
     return acc;
 }
 
+// The same two sums with every load hoisted, for the streaming kernel, where each thread's loads should all be in
+// flight at once.  Every load is in bounds (a missing neighbour reads the cell itself, face fractions exist on all n+1 layers), so all
+// of them can be in flight at once; the terms of domain faces are then left out of the sum, in the reference's order.
+template <class X>
+__device__ __forceinline__ float lap_acc_hoisted(const hf_scene& S, const X& x, float xc, int t, int i, int j, int k) {
+    const int n = S.n, nn = n * n;
+    const bool in0 = i > 0, in1 = i < n - 1, in2 = j > 0, in3 = j < n - 1, in4 = k > 0, in5 = k < n - 1;
+    const float x0 = x(in0 ? t - nn : t), x1 = x(in1 ? t + nn : t), x2 = x(in2 ? t - n : t), x3 = x(in3 ? t + n : t),
+                x4 = x(in4 ? t - 1 : t), x5 = x(in5 ? t + 1 : t);
+    const float a0 = __ldg(S.ax + uidx_(n, i, j, k)), a1 = __ldg(S.ax + uidx_(n, i + 1, j, k)),
+                a2 = __ldg(S.ay + vidx_(n, i, j, k)), a3 = __ldg(S.ay + vidx_(n, i, j + 1, k)),
+                a4 = __ldg(S.az + widx_(n, i, j, k)), a5 = __ldg(S.az + widx_(n, i, j, k + 1));
+    float acc = 0.0f;
+    if (in0) acc = __fadd_rn(acc, __fmul_rn(a0, __fsub_rn(xc, x0)));
+    if (in1) acc = __fadd_rn(acc, __fmul_rn(a1, __fsub_rn(xc, x1)));
+    if (in2) acc = __fadd_rn(acc, __fmul_rn(a2, __fsub_rn(xc, x2)));
+    if (in3) acc = __fadd_rn(acc, __fmul_rn(a3, __fsub_rn(xc, x3)));
+    if (in4) acc = __fadd_rn(acc, __fmul_rn(a4, __fsub_rn(xc, x4)));
+    if (in5) acc = __fadd_rn(acc, __fmul_rn(a5, __fsub_rn(xc, x5)));
+    return acc;
+}
+
+// heat.py:55-91 neighbour_terms with use_fixed = 0; kappa_f from the precomputed face diffusivities (loads hoisted
+// and kept in bounds as in lap_acc)
+template <class X>
+__device__ __forceinline__ float heat_nt_hoisted(const hf_scene& S, const X& x, float xc, int t, int i, int j, int k) {
+    const int n = S.n, nn = n * n;
+    const uint8_t* __restrict__ fl = S.cell_flags;
+    const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
+    const int step[6] = {-nn, nn, -n, n, -1, 1};
+    const int fidx[6] = {uidx_(n, i, j, k), uidx_(n, i + 1, j, k), vidx_(n, i, j, k), vidx_(n, i, j + 1, k),
+                         widx_(n, i, j, k), widx_(n, i, j, k + 1)};
+    const float* __restrict__ hk[3] = {S.hkx, S.hky, S.hkz};
+    float xn[6], kf[6];
+    uint8_t fn[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        const int nb = in[s] ? t + step[s] : t;
+        xn[s] = x(nb);
+        fn[s] = __ldg(fl + nb);
+        kf[s] = __ldg(hk[s >> 1] + fidx[s]);
+    }
+    float acc = 0.0f;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        if (!in[s]) continue;
+        acc = __fadd_rn(acc, (fn[s] & 1) ? __fmul_rn(kf[s], xc) : __fmul_rn(kf[s], __fsub_rn(xc, xn[s])));
+    }
+    return acc;
+}
+
 // heat.py:121-144 k_heat_diag: sum of the in-domain face diffusivities
 __device__ __forceinline__ float heat_diag_sum(const hf_scene& S, int i, int j, int k) {
     const int n = S.n;
@@ -317,82 +368,49 @@ __device__ __forceinline__ void write_stats(const hf_scene& S, const LocalScene&
 }
 
 // ================================================================================================== streaming
-// Scene scalars live in the scene's control record; only the scene's owner block (scene s -> block s % gridDim.x)
-// writes it, in the reduction steps between phases, and every block reads it after the next grid barrier.
-__device__ __forceinline__ LocalScene ctl_load(const CgCtl* c) {
-    LocalScene L;
-    L.bb = __ldcg(&c->bb);
-    L.rr = __ldcg(&c->rr);
-    L.rz = __ldcg(&c->rz);
-    L.pAp = __ldcg(&c->pAp);
-    L.atol_sq = __ldcg(&c->atol_sq);
-    L.mean = __ldcg(&c->mean);
-    L.alpha = __ldcg(&c->alpha);
-    L.beta = __ldcg(&c->beta);
-    L.iters = __ldcg(&c->iters);
-    L.live = __ldcg(&c->live);
-    L.status = __ldcg(&c->status);
-    L.maxit = __ldcg(&c->maxit);
-    return L;
-}
-
-__device__ __forceinline__ void ctl_store(CgCtl* c, const LocalScene& L) {
-    c->bb = L.bb;
-    c->rr = L.rr;
-    c->rz = L.rz;
-    c->pAp = L.pAp;
-    c->atol_sq = L.atol_sq;
-    c->mean = L.mean;
-    c->alpha = L.alpha;
-    c->beta = L.beta;
-    c->iters = L.iters;
-    c->live = L.live;
-    c->status = L.status;
-    c->maxit = L.maxit;
-}
-
-// Tiles are dealt round-robin (tile c to block c % gridDim.x), so every block holds an equal share of every live
-// scene and stays busy while scenes converge at different iterations.  Per iteration:
-//   phase A (tiles of live scenes) | barrier | owners: pAp -> alpha | barrier |
-//   phase B (tiles of live scenes) | barrier | owners: r.r, r.z -> beta, convergence | barrier
+// A launch solves the groups of a GroupTable: consecutive scenes whose CG vectors the host sized to stay in L2.  The
+// grid is split into gt.lanes lanes of equal size (lane = blockIdx.x / blocks per lane), each with its own barrier;
+// a lane takes the next unsolved group from a queue counter, so independent groups run side by side and one lane's
+// barrier waits overlap another lane's stencils on the same SM.  Inside a group, tiles are dealt round-robin over the
+// lane's blocks (an equal share of every live scene per block while scenes converge at different iterations); every
+// block sums the tile partials of every scene of the group itself (same bits everywhere) and keeps the scalars in
+// shared memory, so an iteration takes two lane barriers.  Returns false when a barrier timed out.
 template <bool HEAT>
-__global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles,
-                                                 int num_tiles, int num_scenes, double dt_d, Workspace ws) {
-    __shared__ double red[6 * 32];
-    __shared__ unsigned char s_par[kMaxScenes];
-    __shared__ unsigned char s_live[kMaxScenes];
-    __shared__ float s_coef[kMaxScenes];   // beta in phase A, alpha in phase B
-    for (int s = threadIdx.x; s < num_scenes; s += kThreads) s_par[s] = (unsigned char)scenes[s].state->parity;
-    unsigned* bar = ws.bar + (HEAT ? 0 : 1);
-    unsigned* live_count = ws.live_count + (HEAT ? 0 : 1);
+__device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, const int4 grp,
+                            int lb, int nlb, unsigned* bar, unsigned& epoch, double dt_d, const Workspace& ws,
+                            double* red, LocalScene* loc, unsigned char* s_par, int* s_any) {
+    const int scene_lo = grp.x, scene_hi = grp.y, tile_lo = grp.z, tile_hi = grp.w;
+    const int ns = scene_hi - scene_lo;
     double* bufA = ws.partA;
     double* bufB = ws.partB;
-    CgCtl* ctl = ws.ctl;
-    unsigned epoch = 0;
     const float dt = (float)dt_d;
     const int lt = threadIdx.x;
-    const int G = gridDim.x;
-    __syncthreads();
+    const int first = tile_lo + lb;
+    bool ok = true;
+    if (threadIdx.x < ns) s_par[threadIdx.x] = (unsigned char)scenes[scene_lo + threadIdx.x].state->parity;
 
     // ---------------------------------------------------------------------------------------- prologue
-    if (!HEAT) {
-        // the pressure rhs mean of every scene (grid.py:238-241), summed by the scene's owner
-        for (int s = blockIdx.x; s < num_scenes; s += G) {
+    for (int q = 0; q < ns; ++q) {
+        const int s = scene_lo + q;
+        if (!HEAT) {
+            // the pressure rhs mean (grid.py:238-241) from the divergence stage's chunk sums
             double m[1];
             const int comp[1] = {0};
             scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[s], ws.chunk_begin[s + 1], comp, m, red);
             const int n = scenes[s].n;
-            if (threadIdx.x == 0) ctl[s].mean = (double)__double2float_rn(m[0] / ((double)n * n * n));
+            if (threadIdx.x == 0) loc[q].mean = (double)__double2float_rn(m[0] / ((double)n * n * n));
+        } else if (threadIdx.x == 0) {
+            loc[q].mean = 0.0;
         }
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
     }
-    for (int c = blockIdx.x; c < num_tiles; c += G) {
+    __syncthreads();
+    for (int c = first; c < tile_hi; c += nlb) {
         const TileItem ti = tiles[c];
         const hf_scene& S = scenes[ti.scene];
-        const int n = S.n, par = s_par[ti.scene];
+        const int n = S.n, par = s_par[ti.scene - scene_lo];
         const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
         const float* x = HEAT ? S.T[par ^ 1] : S.p;
-        const float mean = HEAT ? 0.0f : (float)__ldcg(&ctl[ti.scene].mean);
+        const float mean = (float)loc[ti.scene - scene_lo].mean;
         double part[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
@@ -415,40 +433,39 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
             bufB[3 * c + 2] = part[2];
         }
     }
-    if (!grid_barrier(bar, epoch, ws.err)) goto finish;
-    for (int s = blockIdx.x; s < num_scenes; s += G) {
+    if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
+    for (int q = 0; q < ns; ++q) {
+        const int s = scene_lo + q;
         const int b = ws.tile_begin[s], e = ws.tile_begin[s + 1];
         double tot[3];
         const int comp[3] = {0, 1, 2};
         scene_sums<3>(bufB, b, e, comp, tot, red);
         if (threadIdx.x == 0) {
             const hf_scene& S = scenes[s];
-            LocalScene L;
-            init_scalars(L, S, HEAT, tot, S.n * S.n * S.n);
-            L.mean = HEAT ? 0.0 : __ldcg(&ctl[s].mean);
-            L.live = L.live && b < e;
-            L.pAp = 0.0;
-            ctl_store(&ctl[s], L);
-            if (L.live) atomicAdd(live_count, 1u);
+            const double mean = loc[q].mean;
+            init_scalars(loc[q], S, HEAT, tot, S.n * S.n * S.n);
+            loc[q].mean = mean;
+            loc[q].live = loc[q].live && b < e;
         }
     }
-    if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+    if (threadIdx.x == 0) {
+        int any = 0;
+        for (int q = 0; q < ns; ++q) any |= loc[q].live;
+        *s_any = any;
+    }
+    __syncthreads();
 
     // ------------------------------------------------------------------------------------------ iterations
-    for (int kit = 1; *(volatile unsigned*)live_count != 0u; ++kit) {
-        for (int s = threadIdx.x; s < num_scenes; s += kThreads) {
-            s_live[s] = (unsigned char)(__ldcg(&ctl[s].live) != 0);
-            s_coef[s] = __ldcg(&ctl[s].beta);
-        }
-        __syncthreads();
+    for (int kit = 1; *s_any; ++kit) {
         // phase A: p_k at the stencil points, Ap = A p_k, p.Ap
-        for (int c = blockIdx.x; c < num_tiles; c += G) {
+        for (int c = first; c < tile_hi; c += nlb) {
             const TileItem ti = tiles[c];
-            if (!s_live[ti.scene]) continue;
+            const LocalScene& L = loc[ti.scene - scene_lo];
+            if (!L.live) continue;
             const hf_scene& S = scenes[ti.scene];
             const int n = S.n;
             const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
-            const Dir P{S.cg_z, S.cg_p[(kit - 1) & 1], s_coef[ti.scene], kit == 1};
+            const Dir P{S.cg_z, S.cg_p[(kit - 1) & 1], L.beta, kit == 1};
             float pc[4], ap[4];
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
@@ -459,9 +476,9 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
                 if (HEAT) {
                     ap[m] = (__ldg(S.cell_flags + cl.t) & 1)
                                 ? pc[m]
-                                : __fadd_rn(pc[m], __fmul_rn(c_dt, heat_nt(S, P, pc[m], cl.t, cl.i, cl.j, cl.k)));
+                                : __fadd_rn(pc[m], __fmul_rn(c_dt, heat_nt_hoisted(S, P, pc[m], cl.t, cl.i, cl.j, cl.k)));
                 } else {
-                    ap[m] = __fdiv_rn(lap_acc(S, P, pc[m], cl.t, cl.i, cl.j, cl.k), hh);
+                    ap[m] = __fdiv_rn(lap_acc_hoisted(S, P, pc[m], cl.t, cl.i, cl.j, cl.k), hh);
                 }
             }
             float* pnew = S.cg_p[kit & 1];
@@ -477,30 +494,30 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
             group_sum<1>(part, red);
             if (lt == 0) bufA[3 * c] = part[0];
         }
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
-        for (int s = blockIdx.x; s < num_scenes; s += G) {
-            if (!s_live[s]) continue;
+        if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
+        for (int q = 0; q < ns; ++q) {
+            if (!loc[q].live) continue;   // uniform: shared value written before the last __syncthreads
+            const int s = scene_lo + q;
             double tot[1];
             const int comp[1] = {0};
             scene_sums<1>(bufA, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
             if (threadIdx.x == 0) {
-                ctl[s].pAp = tot[0];
-                ctl[s].alpha = __double2float_rn(__ldcg(&ctl[s].rz) / tot[0]);
+                loc[q].pAp = tot[0];
+                loc[q].alpha = __double2float_rn(loc[q].rz / tot[0]);
             }
         }
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
-        for (int s = threadIdx.x; s < num_scenes; s += kThreads) s_coef[s] = __ldcg(&ctl[s].alpha);
         __syncthreads();
         // phase B: x += alpha p, r -= alpha Ap, z = D r, r.r and r.z
-        for (int c = blockIdx.x; c < num_tiles; c += G) {
+        for (int c = first; c < tile_hi; c += nlb) {
             const TileItem ti = tiles[c];
-            if (!s_live[ti.scene]) continue;
+            const LocalScene& L = loc[ti.scene - scene_lo];
+            if (!L.live) continue;
             const hf_scene& S = scenes[ti.scene];
-            const int n = S.n, par = s_par[ti.scene];
+            const int n = S.n, par = s_par[ti.scene - scene_lo];
             float* x = HEAT ? S.T[par ^ 1] : S.p;
             const float* D = HEAT ? S.hdiag : S.pdiag;
             const float* pk = S.cg_p[kit & 1];
-            const float alpha = s_coef[ti.scene];
+            const float alpha = L.alpha;
             float xv[4], rv[4], zv[4];
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
@@ -528,26 +545,28 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
                 bufB[3 * c + 2] = part[1];
             }
         }
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
-        for (int s = blockIdx.x; s < num_scenes; s += G) {
-            if (!s_live[s]) continue;
+        if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
+        for (int q = 0; q < ns; ++q) {
+            if (!loc[q].live) continue;
+            const int s = scene_lo + q;
             double tot[2];
             const int comp[2] = {1, 2};
             scene_sums<2>(bufB, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
-            if (threadIdx.x == 0) {
-                LocalScene L = ctl_load(&ctl[s]);
-                if (!update_scalars(L, HEAT, tot[0], tot[1], kit)) atomicSub(live_count, 1u);
-                ctl_store(&ctl[s], L);
-            }
+            if (threadIdx.x == 0) update_scalars(loc[q], HEAT, tot[0], tot[1], kit);
         }
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        if (threadIdx.x == 0) {
+            int any = 0;
+            for (int q = 0; q < ns; ++q) any |= loc[q].live;
+            *s_any = any;
+        }
+        __syncthreads();
     }
     // -------------------------------------------------------------------- pressure epilogue: projection
     if (!HEAT) {
-        for (int c = blockIdx.x; c < num_tiles; c += G) {
+        for (int c = first; c < tile_hi; c += nlb) {
             const TileItem ti = tiles[c];
             const hf_scene& S = scenes[ti.scene];
-            const int n = S.n, par = s_par[ti.scene];
+            const int n = S.n, par = s_par[ti.scene - scene_lo];
             const float h = (float)S.h, dtr = (float)(dt_d / S.rho);
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
@@ -556,16 +575,45 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
             }
         }
     }
-finish:
-    // Every block read the parities before its first barrier, so block 0 may flip them now; the control records were
-    // final at the last barrier.
-    if (blockIdx.x == 0) {
-        const bool timed_out = *(volatile int*)ws.err != 0;
-        for (int s = threadIdx.x; s < num_scenes; s += kThreads) {
-            const hf_scene& S = scenes[s];
-            if (!(S.flags & HF_FLAG_ACTIVE)) continue;
-            write_stats(S, ctl_load(&ctl[s]), HEAT, timed_out, s_par[s]);
+done:
+    // Every block of the lane read the group's parities before its first barrier, so the lane's first block may
+    // flip them now (the lane's other blocks may already be in the next group: other scenes).
+    __syncthreads();
+    if (lb == 0) {
+        for (int q = threadIdx.x; q < ns; q += kThreads) {
+            const hf_scene& S = scenes[scene_lo + q];
+            if (S.flags & HF_FLAG_ACTIVE) write_stats(S, loc[q], HEAT, !ok, s_par[q]);
         }
+    }
+    __syncthreads();
+    return ok;
+}
+
+template <bool HEAT>
+__global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles,
+                                                 double dt_d, Workspace ws, const __grid_constant__ GroupTable gt) {
+    __shared__ double red[6 * 32];
+    __shared__ LocalScene loc[kGroupScenes];
+    __shared__ unsigned char s_par[kGroupScenes];
+    __shared__ int s_any;
+    const int nlb = gridDim.x / gt.lanes;           // blocks per lane (the host launches a multiple of gt.lanes)
+    const int lane = blockIdx.x / nlb, lb = blockIdx.x % nlb;
+    unsigned* bar = ws.bar + (HEAT ? 0 : kMaxLanes) + lane;
+    int* next = ws.lane_next + (HEAT ? 0 : kMaxLanes) + lane;
+    unsigned* queue = ws.queue + (HEAT ? 0 : 1);
+    unsigned epoch = 0;
+    for (;;) {
+        if (lb == 0 && threadIdx.x == 0) *(volatile int*)next = (int)atomicAdd(queue, 1u);
+        if (!grid_barrier(bar, epoch, ws.err, nlb)) break;
+        const int g = *(volatile int*)next;
+        if (g >= gt.count) break;
+        if (!solve_group<HEAT>(scenes, tiles, gt.g[g], lb, nlb, bar, epoch, dt_d, ws, red, loc, s_par, &s_any)) break;
+    }
+    // a timed-out barrier leaves the groups that no lane reached unsolved: flag their scenes
+    if (blockIdx.x == 0 && *(volatile int*)ws.err) {
+        for (int q = 0; q < gt.count; ++q)
+            for (int s = gt.g[q].x + (int)threadIdx.x; s < gt.g[q].y; s += kThreads)
+                if (scenes[s].flags & HF_FLAG_ACTIVE) scenes[s].state->status |= HF_SCENE_BARRIER_TIMEOUT;
     }
 }
 
@@ -615,7 +663,7 @@ __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, 
 // Block = `groups` x 256 threads; group g owns tiles c0 + g + groups*q (q < MAXC) of the block's contiguous range.
 template <bool HEAT, int MAXC, bool TMA>
 __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
-    k_pcg_res(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int num_tiles, int num_scenes,
+    k_pcg_res(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int tile_lo, int tile_hi,
               double dt_d, Workspace ws, const __grid_constant__ TileMaps maps) {
     constexpr int CPT = 4 * MAXC;   // cells per thread
     extern __shared__ __align__(128) float sm_raw[];
@@ -625,13 +673,13 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     __shared__ LocalScene Ls;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
     const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
-    const int c0 = (int)(((long long)num_tiles * blockIdx.x) / gridDim.x);
-    const int c1 = (int)(((long long)num_tiles * (blockIdx.x + 1)) / gridDim.x);
+    const int c0 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * blockIdx.x) / gridDim.x);
+    const int c1 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * (blockIdx.x + 1)) / gridDim.x);
     const int sidx = tiles[c0].scene;   // one scene per plan on this path
     const hf_scene& S = scenes[sidx];
     const int n = S.n, N = n * n * n;
     const int par = S.state->parity;
-    unsigned* bar = ws.bar + (HEAT ? 0 : 1);
+    unsigned* bar = ws.bar + (HEAT ? 0 : kMaxLanes);
     unsigned epoch = 0;
     const float dt = (float)dt_d;
     const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
@@ -714,7 +762,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         if (!ok) atomicExch(ws.err, 1);
         phase_bit ^= 1u;
     }
-    if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+    if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
     {
         double tot[3];
         const int comp[3] = {0, 1, 2};
@@ -829,7 +877,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             const int c = c0 + g + groups * q;
             if (lt == 0 && have[q]) bufA[3 * c] = part[0];
         }
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
         {
             double tot[1];
             const int comp[1] = {0};
@@ -864,7 +912,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 bufB[3 * c + 2] = part[1];
             }
         }
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
         {
             double tot[2];
             const int comp[2] = {1, 2};
@@ -884,7 +932,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     }
     if (!HEAT) {
         // grid.py:140-153: the projection reads p at neighbour cells owned by other blocks
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
         const float dtr = (float)(dt_d / S.rho);
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) {
@@ -913,7 +961,7 @@ finish:
 // thread's tiles.
 template <int MAXC>
 __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
-    k_pcg_tma(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int num_tiles, int num_scenes,
+    k_pcg_tma(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int tile_lo, int tile_hi,
               double dt_d, Workspace ws, const __grid_constant__ TileMaps maps) {
     constexpr int CPT = 4 * MAXC;
     extern __shared__ __align__(128) float sm_raw[];
@@ -922,13 +970,13 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     __shared__ LocalScene Ls;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
     const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
-    const int c0 = (int)(((long long)num_tiles * blockIdx.x) / gridDim.x);
-    const int c1 = (int)(((long long)num_tiles * (blockIdx.x + 1)) / gridDim.x);
+    const int c0 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * blockIdx.x) / gridDim.x);
+    const int c1 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * (blockIdx.x + 1)) / gridDim.x);
     const int sidx = tiles[c0].scene;
     const hf_scene& S = scenes[sidx];
     const int n = S.n, N = n * n * n;
     const int par = S.state->parity;
-    unsigned* bar = ws.bar + 1;
+    unsigned* bar = ws.bar + kMaxLanes;
     unsigned epoch = 0;
     const float h = (float)S.h, hh = __fmul_rn(h, h);
     double* bufA = ws.partA;
@@ -1015,7 +1063,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         if (!ok) atomicExch(ws.err, 1);
         phase_bit ^= 1u;
     }
-    if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+    if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
     {
         double tot[3];
         const int comp[3] = {0, 1, 2};
@@ -1105,7 +1153,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 if (lt == 0 && have[q]) bufA[3 * c] = part[q];
             }
         }
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
         {
             double tot[1];
             const int comp[1] = {0};
@@ -1148,7 +1196,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 }
             }
         }
-        if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+        if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
         {
             double tot[2];
             const int comp[2] = {1, 2};
@@ -1166,7 +1214,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             if (have[q] && cl.ok) xg[cl.t] = x[q * 4 + m];
         }
     }
-    if (!grid_barrier(bar, epoch, ws.err)) goto finish;
+    if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
     {
         const float dtr = (float)(dt_d / S.rho);
 #pragma unroll

@@ -15,10 +15,21 @@ struct CgCtl {
     int iters, live, status, maxit;
 };
 
+constexpr int kMaxLanes = 8;      // lanes of one streaming CG launch
+constexpr int kGroupScenes = 32;  // scenes of one CG group (every block of a lane keeps all their scalars)
+constexpr int kMaxGroups = 1024;  // groups of one launch (a kernel parameter: 16 KB)
+
+// Scene groups of a streaming CG launch: group q = scenes [g[q].x, g[q].y), tiles [g[q].z, g[q].w).
+struct GroupTable {
+    int count, lanes;
+    int4 g[kMaxGroups];
+};
+
 // Device pointers into the caller's workspace buffer (see hf_api.cu: workspace_layout).
 struct Workspace {
-    unsigned* bar;          // [2] grid-barrier counters (reset before every persistent launch)
-    unsigned* live_count;   // [2] scenes still iterating
+    unsigned* bar;          // [2 kMaxLanes] barrier counters: heat lanes, then pressure lanes (reset every launch)
+    unsigned* queue;        // [2] next group to solve (heat, pressure)
+    int* lane_next;         // [2 kMaxLanes] group a lane works on
     int* err;               // [1] barrier timeout flag
     int* chunk_begin;       // [S+1] first chunk of every scene in the chunk table
     int* tile_begin;        // [S+1] first tile of every scene in the tile table
@@ -52,11 +63,13 @@ __global__ void k_laplacian_plain(int n, float h, float alpha, float beta, const
 __global__ void k_heat_matvec_plain(int n, float h, float dt, float alpha, float beta, const float* __restrict__ x,
                                     const float* __restrict__ kap, const uint8_t* __restrict__ fl,
                                     const float* __restrict__ y, float* __restrict__ out);
-// persistent cooperative Jacobi-PCG kernel (heat = heat system, else pressure system + projection + end of substep);
-// arguments: (const hf_scene*, const TileItem*, int num_tiles, int num_scenes, double dt, Workspace)
+// persistent cooperative Jacobi-PCG kernel over the groups of a GroupTable (heat = heat system, else pressure system +
+// projection + end of substep); arguments: (const hf_scene*, const TileItem*, double dt, Workspace, GroupTable); the
+// grid is a multiple of the table's lanes
 const void* pcg_kernel(bool heat);
 // register-resident single-scene variant (MAXC tiles per 256-thread group: 1, 2 or 3; blockDim = 256 x groups);
-// arguments as pcg_kernel plus a TileMaps (used when tma); dynamic shared memory pcg_resident_smem(...)
+// arguments: (const hf_scene*, const TileItem*, int tile_lo, int tile_hi, double dt, Workspace, TileMaps) -- the
+// scene's tiles; the TileMaps is used when tma; dynamic shared memory pcg_resident_smem(...)
 const void* pcg_resident_kernel(bool heat, int maxc, bool tma);
 size_t pcg_resident_smem(int groups, int maxc, bool tma);
 // device addresses of the per-scene chunk and tile offset tables inside a plan's workspace

@@ -274,7 +274,6 @@ __global__ void __launch_bounds__(kThreads) k_advect_T(const hf_scene* __restric
     float* T2 = S.T[par ^ 1];
     const float h = (float)S.h, dt = (float)dt_d;
     const float* Tw = S.Tw;
-    const float* kap = S.kap;
     const uint8_t* fl = S.cell_flags;
     const float c_dt = __fdiv_rn(dt, __fmul_rn(h, h));
     for (int m = 0; m < kCellsPerThread; ++m) {

@@ -17,6 +17,7 @@ HF_SCENE_HEAT_MAXITER, HF_SCENE_PRESSURE_MAXITER, HF_SCENE_NONFINITE, HF_SCENE_B
 CHUNK = 1024
 HF_PLAN_STREAMING_CG = 1
 HF_PLAN_NO_TMA = 2
+HF_PLAN_LANES_SHIFT = 8
 
 _P = C.c_void_p
 
@@ -49,7 +50,7 @@ class Scene(C.Structure):
 
 
 class Plan(C.Structure):
-    _fields_ = [("num_scenes", C.c_int32), ("num_chunks", C.c_int32), ("num_tiles", C.c_int32), ("reserved_t", C.c_int32),
+    _fields_ = [("num_scenes", C.c_int32), ("num_chunks", C.c_int32), ("num_tiles", C.c_int32), ("group_cells", C.c_int32),
                 ("tiles_dev", _P), ("scenes_host", _P), ("scenes_dev", _P),
                 ("work_dev", _P), ("workspace", _P), ("workspace_bytes", C.c_size_t), ("persistent_blocks", C.c_int32),
                 ("options", C.c_int32)]

@@ -6,9 +6,10 @@ so scenes of different n share every launch), optionally captures K substeps in 
 state.  The CG solves of a batch run in the streaming persistent kernels with per-scene convergence masking: a scene
 that has converged stops iterating while the others continue.  Results are bit-identical to each scene run alone.
 
-``autotune`` picks the persistent-kernel grid (blocks per SM) for a batch by timing candidates on the device; every
-candidate computes the same bits, so tuning never changes results.  Choices are cached per GPU and batch signature in
-a JSON file.
+``autotune`` picks the launch shape of the CG solves for a batch -- blocks of the streaming kernel, the cells of one
+scene group (a group's CG vectors should stay in L2) and the lanes that solve groups side by side -- by timing
+candidates on the device; every candidate computes the same bits, so tuning never changes results.  Choices are cached
+per GPU and batch signature in a JSON file.
 """
 from __future__ import annotations
 
@@ -123,11 +124,12 @@ def make_scene(sc: AirScenario, device="cuda:0") -> DeviceScene:
 class AirBatch:
     """Scenes advanced together by one plan; see the module docstring."""
 
-    def __init__(self, scenarios, device="cuda:0", persistent_blocks=0, scenes=None):
+    def __init__(self, scenarios, device="cuda:0", persistent_blocks=0, scenes=None, group_cells=0, lanes=0):
         self.device = torch.device(device)
         self.scenarios = list(scenarios)
         self.scenes = scenes if scenes is not None else [make_scene(s, device) for s in self.scenarios]
-        self.plan = ScenePlan(self.scenes, device, persistent_blocks=persistent_blocks)
+        self.plan = ScenePlan(self.scenes, device, persistent_blocks=persistent_blocks, group_cells=group_cells,
+                              lanes=lanes)
         self.plan.prepare_statics()
         self.graph = None
         self._graph_key = None
@@ -184,11 +186,12 @@ def _signature(scenes):
 
 
 def autotune(batch: AirBatch, dt=2e-3, reps=3, candidates=None, cache=True):
-    """Time the persistent-grid candidates (blocks per SM of the streaming CG kernels) on this batch and keep the
-    fastest.  Returns (chosen persistent_blocks, {candidate: ms per substep})."""
+    """Time launch-shape candidates (persistent_blocks, group_cells, lanes) of the CG solves on this batch and keep
+    the fastest.  Returns (the chosen triple, {"blocks/cells/lanes": ms per substep})."""
     sms = torch.cuda.get_device_properties(batch.device).multi_processor_count
     name = torch.cuda.get_device_name(batch.device)
     key = f"{name}|{_signature(batch.scenes)}"
+    plan = batch.plan
     table = {}
     if cache and os.path.exists(_CACHE):
         try:
@@ -196,13 +199,14 @@ def autotune(batch: AirBatch, dt=2e-3, reps=3, candidates=None, cache=True):
         except ValueError:
             table = {}
     if cache and key in table:
-        pb = int(table[key]["persistent_blocks"])
-        batch.plan.plan.persistent_blocks = pb
-        return pb, table[key]["timings"]
-    candidates = candidates or [sms, 2 * sms, 3 * sms, 4 * sms]
+        best = tuple(int(v) for v in table[key]["choice"])
+        plan.plan.persistent_blocks, plan.plan.group_cells, plan.lanes = best
+        return best, table[key]["timings"]
+    candidates = candidates or [(b * sms, g, l) for (g, l) in ((0, 1), (0, 2), (1, 4), (0, 4))
+                                for b in (2, 4, 5)]
     timings = {}
-    for pb in candidates:
-        batch.plan.plan.persistent_blocks = pb
+    for pb, gc, ln in candidates:
+        plan.plan.persistent_blocks, plan.plan.group_cells, plan.lanes = pb, gc, ln
         batch.plan.substep(dt)                       # warm-up
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
@@ -210,16 +214,17 @@ def autotune(batch: AirBatch, dt=2e-3, reps=3, candidates=None, cache=True):
             batch.plan.substep(dt)
         b.record()
         torch.cuda.synchronize()
-        timings[pb] = a.elapsed_time(b) / reps
+        timings[(pb, gc, ln)] = a.elapsed_time(b) / reps
     best = min(timings, key=timings.get)
-    batch.plan.plan.persistent_blocks = best
+    plan.plan.persistent_blocks, plan.plan.group_cells, plan.lanes = best
+    out = {"/".join(str(v) for v in k): t for k, t in timings.items()}
     if cache:
-        table[key] = {"persistent_blocks": best, "timings": {str(k): v for k, v in timings.items()}}
+        table[key] = {"choice": list(best), "timings": out}
         try:
             json.dump(table, open(_CACHE, "w"), indent=1)
         except OSError:
             pass
-    return best, timings
+    return best, out
 
 
 def shard_scenarios(scenarios, rank, world):

@@ -215,7 +215,8 @@ class DeviceScene:
 class ScenePlan:
     """Scene table + work table + workspace for a list of DeviceScene, and the stage calls over them."""
 
-    def __init__(self, scenes, device="cuda:0", persistent_blocks=0, streaming_cg=False, tma=True):
+    def __init__(self, scenes, device="cuda:0", persistent_blocks=0, streaming_cg=False, tma=True, group_cells=0,
+                 lanes=0):
         self.L = _lib.load()
         self.scenes = list(scenes)
         self.device = torch.device(device)
@@ -239,8 +240,21 @@ class ScenePlan:
         self.plan.workspace = self.workspace.data_ptr()
         self.plan.workspace_bytes = ws_bytes
         self.plan.persistent_blocks = persistent_blocks
+        self.plan.group_cells = group_cells
         self.plan.options = (_lib.HF_PLAN_STREAMING_CG if streaming_cg else 0) | (0 if tma else _lib.HF_PLAN_NO_TMA)
+        self.lanes = lanes
         self.upload()
+
+    @property
+    def lanes(self):
+        """Lanes of the streaming CG launch: independent scene groups solved side by side (0 or 1: one lane)."""
+        return (self.plan.options >> _lib.HF_PLAN_LANES_SHIFT) & 15
+
+    @lanes.setter
+    def lanes(self, k):
+        if not 0 <= int(k) <= 8:
+            raise ValueError("lanes must be 0..8")
+        self.plan.options = (self.plan.options & ~(15 << _lib.HF_PLAN_LANES_SHIFT)) | (int(k) << _lib.HF_PLAN_LANES_SHIFT)
 
     def stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)

@@ -54,13 +54,15 @@ def poisson_trace(rate=20.0, duration=60.0, seed=0, edges=(48, 64, 96, 128), hor
 
 
 class AirServer:
-    def __init__(self, device="cuda:0", dt=2e-3, hbm_budget=150e9, max_slots=256, persistent_blocks=0,
-                 keep_results=False, result_fields=("T",)):
+    def __init__(self, device="cuda:0", dt=2e-3, hbm_budget=150e9, max_slots=256, persistent_blocks=0, group_cells=0,
+                 lanes=0, keep_results=False, result_fields=("T",)):
         self.device = torch.device(device)
         self.dt = dt
         self.budget = float(hbm_budget)
         self.max_slots = max_slots
         self.persistent_blocks = persistent_blocks
+        self.group_cells = group_cells
+        self.lanes = lanes
         self.keep_results = keep_results
         self.result_fields = ("T", "u", "v", "w") if keep_results else tuple(result_fields)
         self.h2d_bytes = 0
@@ -118,8 +120,8 @@ class AirServer:
 
     # ------------------------------------------------------------------------------------------------ stepping
     def _rebuild(self):
-        self.plan = ScenePlan([r.scene for r in self.active], self.device, persistent_blocks=self.persistent_blocks) \
-            if self.active else None
+        self.plan = ScenePlan([r.scene for r in self.active], self.device, persistent_blocks=self.persistent_blocks,
+                              group_cells=self.group_cells, lanes=self.lanes) if self.active else None
         self.plan_builds += 1
 
     def step(self, now):

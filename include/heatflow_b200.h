@@ -113,13 +113,16 @@ typedef struct hf_scene {
 #define HF_PLAN_STREAMING_CG 1u      /* never use the register-resident CG variant (single-scene plans use it when
                                         the scene's tiles fit one block per SM) */
 #define HF_PLAN_NO_TMA 2u            /* resident pressure CG without the TMA-staged stencil */
+#define HF_PLAN_LANES_SHIFT 8        /* options bits 8..11: lanes of the streaming CG launch (independent scene groups
+                                        solved side by side, each lane with its own barrier; 0 = one lane) */
 
 /* A batch of scenes ready to launch: tables in device memory plus the host copy used to size launches. */
 typedef struct hf_plan {
     int32_t num_scenes;
     int32_t num_chunks;        /* 1024-cell work items over all scenes */
     int32_t num_tiles;         /* 4 x 8 x 32-cell tiles over all scenes (work items of the CG solves) */
-    int32_t reserved_t;
+    int32_t group_cells;       /* most cells of one CG group of the streaming solve (0 = a default that keeps a group's
+                                  CG vectors in L2) */
     void *tiles_dev;           /* device: int32 quadruples (scene, i0, j0, k0) [num_tiles] */
     const hf_scene *scenes_host;   /* host copy, valid while the plan is used */
     void *scenes_dev;          /* device: hf_scene[num_scenes] */
