@@ -75,7 +75,7 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="served: length of the trace window")
     ap.add_argument("--rate", type=float, default=20.0, help="served: mean arrivals per second")
     ap.add_argument("--hbm-budget", type=float, default=150e9, help="served: HBM admitted for scenes, bytes")
-    ap.add_argument("--max-slots", type=int, default=256, help="served: most scenes in one batch")
+    ap.add_argument("--max-slots", type=int, default=64, help="served: most scenes in one batch")
     return ap.parse_args()
 
 
@@ -338,7 +338,7 @@ def bench_plain(args, dev, rank, world, local):
     except (OSError, ValueError, KeyError):
         pass
     roof = roofline(cg_bytes / (cg_ms / steps / 1000.0) / 1e9, peaks, traffic=traffic,
-                    kernel="k_pcg_tma<1> (pressure Jacobi-PCG + projection, one persistent cooperative launch, "
+                    kernel="k_pcg_tma<2> (pressure Jacobi-PCG + projection, one persistent cooperative launch, "
                            "TMA-staged register-resident stencil)",
                     bytes_per_launch=cg_bytes, ms_per_launch=cg_ms / steps, mean_pressure_iters=p_iters / steps)
     sb = substep_bytes(N, h_iters / steps, p_iters / steps, True)
