@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--ref-seconds", type=float, default=60.0, help="budget of the timed CPU reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="plain line without the batched/served summaries")
+    ap.add_argument("--resident-tiles", type=int, default=0, help="plain: tiles per group of the resident CG (0: auto)")
     ap.add_argument("--scenes", type=int, default=64, help="batched: scenes in the ensemble")
     ap.add_argument("--graph-steps", type=int, default=10, help="batched: substeps per captured CUDA graph")
     ap.add_argument("--edges", default="32,48,64,96,128", help="batched: grid edges the ensemble draws from")
@@ -267,6 +268,22 @@ def roofline(achieved_gbs, peaks, **extra):
     return out
 
 
+def stage_breakdown(plan, stages, substeps=20):
+    """Mean device time of every stage of a substep, from CUDA events around each stage launch over `substeps`
+    substeps run after the timed region (the stages in substep order, warm caches as in the timed run)."""
+    import torch
+    ev = {nm: [] for nm, _ in stages}
+    for _ in range(substeps):
+        for nm, fn in stages:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            ev[nm].append((a, b))
+    torch.cuda.synchronize()
+    return {nm: sum(a.elapsed_time(b) for a, b in v) / len(v) for nm, v in ev.items()}
+
+
 # --------------------------------------------------------------------------------------------------- plain
 def bench_plain(args, dev, rank, world, local):
     import torch
@@ -274,6 +291,7 @@ def bench_plain(args, dev, rank, world, local):
     steps = args.steps if args.steps is not None else 1000
     sim = coupled_default(device=dev)
     sc, plan = sim.scene, sim.plan
+    plan.resident_tiles = args.resident_tiles
     n = sim.grid.n
     N = n ** 3
     stream = torch.cuda.current_stream()
@@ -313,6 +331,10 @@ def bench_plain(args, dev, rank, world, local):
     value = world * steps / (el_ms / 1000.0)
     # footprint, scatter, obstacle, coeff, prestage, advect_T, heat CG, particle update, face, divergence, pressure CG
     launches_per_step = 11
+    stage_ms = stage_breakdown(plan, [("obstacle", plan.obstacle_fields), ("temperature", lambda: plan.temperature_stage(DT)),
+                                      ("heat_cg", lambda: plan.heat_solve(DT)), ("particles", plan.particle_update),
+                                      ("face", lambda: plan.face_stage(DT)), ("divergence", lambda: plan.divergence_stage(DT)),
+                                      ("pressure_cg", lambda: plan.pressure_cg(DT))])
     # ---- end to end through the public API: pinned H2D of the particle state, D2H of grid_T, every substep
     pos_h = sim.body.pos_t.cpu().pin_memory()
     vel_h = sim.body.vel_t.cpu().pin_memory()
@@ -366,7 +388,7 @@ def bench_plain(args, dev, rank, world, local):
                              "(~35 MB) stays L2-resident within a substep by design",
                        "mean_pressure_iters": p_iters / steps, "mean_heat_iters": h_iters / steps,
                        "cell_updates_per_s": value * N, "substep_status": int(st1.status),
-                       "substep_roofline": sub_roof},
+                       "substep_roofline": sub_roof, "stage_ms": stage_ms},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * steps, "clocks": ck}
 
 

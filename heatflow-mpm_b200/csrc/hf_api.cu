@@ -39,6 +39,9 @@ struct DeviceInfo {
     int occ_heat = 0, occ_pressure = 0;
     size_t smem_optin = 0;
     bool ready = false;
+    // occupancy of each resident variant [heat][tiles per group][tma][groups] (-1: not queried yet; the query also
+    // raises the kernel's dynamic shared-memory limit)
+    int res_occ[2][4][2][5];
 };
 
 constexpr int kResGroupsMax[4] = {0, 4, 3, 2};   // 256-thread groups per block of the resident variant, by MAXC
@@ -65,6 +68,7 @@ int device_info(DeviceInfo** out) {
         HF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "cudaDeviceGetAttribute");
         d.smem_optin = (size_t)optin;
         if (!d.coop) return fail(HF_ERR_DEVICE, "device does not support cooperative launches");
+        std::memset(d.res_occ, 0xff, sizeof d.res_occ);
         d.ready = true;
     }
     *out = &d;
@@ -160,7 +164,7 @@ bool any_flag(const hf_plan* p, unsigned f) {
 
 // The resident variant for a plan with one active scene whose tiles fit one block per SM.  Returns HF_OK after
 // launching, or -1 when the scene does not fit (the caller falls back to the streaming kernel).
-int launch_resident(const hf_plan* p, const DeviceInfo* d, bool heat, double dt, int s, void* stream) {
+int launch_resident(const hf_plan* p, DeviceInfo* d, bool heat, double dt, int s, void* stream) {
     hf::Workspace ws = workspace(p);
     const hf_scene* scenes = static_cast<const hf_scene*>(p->scenes_dev);
     const hf::TileItem* tiles = static_cast<const hf::TileItem*>(p->tiles_dev);
@@ -170,16 +174,21 @@ int launch_resident(const hf_plan* p, const DeviceInfo* d, bool heat, double dt,
     const int G = nt < d->sms ? nt : d->sms;
     const int tpb = (nt + G - 1) / G;
     const bool tma = !heat && (sc.n % 4 == 0) && !(p->options & HF_PLAN_NO_TMA);
-    for (int m = 1; m <= 3; ++m) {
+    const int want = (int)((p->options >> HF_PLAN_RES_TILES_SHIFT) & 3u);   // 0: the first that fits
+    for (int m = want ? want : 1; m <= 3; ++m) {
         const int groups = (tpb + m - 1) / m;
         if (groups > kResGroupsMax[m]) continue;
         const void* fn = hf::pcg_resident_kernel(heat, m, tma);
         const size_t smem = hf::pcg_resident_smem(groups, m, tma);
         if (smem > d->smem_optin) continue;
-        if (smem > 48 * 1024)
-            HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
-        int occ = 0;
-        HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256 * groups, smem), "occupancy (resident)");
+        int& occ = d->res_occ[heat][m][tma][groups];
+        if (occ < 0) {
+            if (smem > 48 * 1024)
+                HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+            int o = 0;
+            HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, 256 * groups, smem), "occupancy (resident)");
+            occ = o;
+        }
         if (occ < 1) continue;
         hf::TileMaps maps;
         std::memset(&maps, 0, sizeof maps);

@@ -33,6 +33,9 @@
 namespace hf {
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;   // 2 s
+// Components one group_sum / scene_sums call reduces at most: 3 inner products per tile x 3 tiles of a 256-thread
+// group (the resident variants' set-up).  Every CG kernel's `red` holds kRedComps x 32 doubles (one per warp).
+constexpr int kRedComps = 9;
 
 __device__ __forceinline__ int uidx_(int n, int i, int j, int k) { return (i * n + j) * n + k; }
 __device__ __forceinline__ int vidx_(int n, int i, int j, int k) { return (i * (n + 1) + j) * n + k; }
@@ -67,6 +70,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& epoch, int
 template <int K, int STRIDE = 3>
 __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b, int e, const int (&comp)[K],
                                            double (&tot)[K], double* red) {
+    static_assert(K <= kRedComps, "red holds kRedComps components");
 #pragma unroll
     for (int q = 0; q < K; ++q) tot[q] = 0.0;
     if (threadIdx.x < kThreads) {
@@ -99,6 +103,7 @@ __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b
 // Per-256-thread-group sum (each group reduces its own 8 warps in index order): the tile partial tree.
 template <int K>
 __device__ __forceinline__ void group_sum(double (&v)[K], double* red) {
+    static_assert(K <= kRedComps, "red holds kRedComps components");
 #pragma unroll
     for (int c = 0; c < K; ++c) {
 #pragma unroll
@@ -592,7 +597,7 @@ done:
 template <bool HEAT>
 __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles,
                                                  double dt_d, Workspace ws, const __grid_constant__ GroupTable gt) {
-    __shared__ double red[6 * 32];
+    __shared__ double red[kRedComps * 32];
     __shared__ LocalScene loc[kGroupScenes];
     __shared__ unsigned char s_par[kGroupScenes];
     __shared__ int s_any;
@@ -669,7 +674,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     extern __shared__ __align__(128) float sm_raw[];
     // TMA destinations must be 128-byte aligned: the launch adds 128 bytes of slack
     float* sm_boxes = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
-    __shared__ double red[6 * 32];
+    __shared__ double red[kRedComps * 32];
     __shared__ LocalScene Ls;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
     const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
@@ -966,7 +971,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     constexpr int CPT = 4 * MAXC;
     extern __shared__ __align__(128) float sm_raw[];
     float* sm_boxes = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
-    __shared__ double red[6 * 32];
+    __shared__ double red[kRedComps * 32];
     __shared__ LocalScene Ls;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
     const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;

@@ -38,12 +38,22 @@ __device__ __forceinline__ float maxf_(float a, float b) { return a > b ? a : b;
 // Warp's clamp(x, lo, hi) = min(max(lo, x), hi)
 __device__ __forceinline__ float clampf_(float x, float lo, float hi) { return minf_(maxf_(lo, x), hi); }
 
+// A sample point in grid units: each coordinate divided by h once (fields.py:14-15 divides before the offset), shared
+// by every lattice sampled at that point.
+struct GridPos {
+    float x, y, z;
+};
+
+__device__ __forceinline__ GridPos grid_pos(float px, float py, float pz, float h) {
+    return GridPos{__fdiv_rn(px, h), __fdiv_rn(py, h), __fdiv_rn(pz, h)};
+}
+
 // fields.py:5-36 -- trilinear sample of an (nx,ny,nz) lattice with nodes at (i + off) h, indices clamped.
-__device__ __forceinline__ float sample(const float* __restrict__ a, float px, float py, float pz, float ox, float oy,
-                                        float oz, float h, int nx, int ny, int nz) {
-    float gx = __fsub_rn(__fdiv_rn(px, h), ox);
-    float gy = __fsub_rn(__fdiv_rn(py, h), oy);
-    float gz = __fsub_rn(__fdiv_rn(pz, h), oz);
+__device__ __forceinline__ float sample_at(const float* __restrict__ a, GridPos q, float ox, float oy, float oz, int nx,
+                                           int ny, int nz) {
+    float gx = __fsub_rn(q.x, ox);
+    float gy = __fsub_rn(q.y, oy);
+    float gz = __fsub_rn(q.z, oz);
     int ix = (int)floorf(gx), iy = (int)floorf(gy), iz = (int)floorf(gz);
     float fx = __fsub_rn(gx, (float)ix), fy = __fsub_rn(gy, (float)iy), fz = __fsub_rn(gz, (float)iz);
     float wx0 = __fsub_rn(1.0f, fx), wy0 = __fsub_rn(1.0f, fy), wz0 = __fsub_rn(1.0f, fz);
@@ -64,13 +74,19 @@ __device__ __forceinline__ float sample(const float* __restrict__ a, float px, f
     return s;
 }
 
-// fields.py:68-72
+__device__ __forceinline__ float sample(const float* __restrict__ a, float px, float py, float pz, float ox, float oy,
+                                        float oz, float h, int nx, int ny, int nz) {
+    return sample_at(a, grid_pos(px, py, pz, h), ox, oy, oz, nx, ny, nz);
+}
+
+// fields.py:68-72 (the three lattices at one point: one division per coordinate)
 __device__ __forceinline__ void sample_velocity(const float* __restrict__ u, const float* __restrict__ v,
                                                 const float* __restrict__ w, float px, float py, float pz, float h, int n,
                                                 float* o) {
-    o[0] = sample(u, px, py, pz, 0.0f, 0.5f, 0.5f, h, n + 1, n, n);
-    o[1] = sample(v, px, py, pz, 0.5f, 0.0f, 0.5f, h, n, n + 1, n);
-    o[2] = sample(w, px, py, pz, 0.5f, 0.5f, 0.0f, h, n, n, n + 1);
+    const GridPos q = grid_pos(px, py, pz, h);
+    o[0] = sample_at(u, q, 0.0f, 0.5f, 0.5f, n + 1, n, n);
+    o[1] = sample_at(v, q, 0.5f, 0.0f, 0.5f, n, n + 1, n);
+    o[2] = sample_at(w, q, 0.5f, 0.5f, 0.0f, n, n, n + 1);
 }
 
 // fields.py:111-116: departure point x - dt u(x - dt/2 u(x))

@@ -336,8 +336,9 @@ __global__ void __launch_bounds__(kThreads) k_particle_update(const hf_scene* __
     const float t_sol = (float)S.t_sol, t_liq = (float)S.t_liq, y_solid = (float)S.y_solid;
     const float mu_s = (float)S.mu_s, mu_l = (float)S.mu_l, t_max = (float)S.t_max;
     const float px = S.pos[3 * t], py = S.pos[3 * t + 1], pz = S.pos[3 * t + 2];
-    const float dT = __fsub_rn(sample(S.T[par ^ 1], px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n),
-                               sample(S.Tw, px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n));
+    const GridPos q = grid_pos(px, py, pz, h);
+    const float dT = __fsub_rn(sample_at(S.T[par ^ 1], q, 0.5f, 0.5f, 0.5f, n, n, n),
+                               sample_at(S.Tw, q, 0.5f, 0.5f, 0.5f, n, n, n));
     const float tp = clampf_(__fadd_rn(S.ptemp[t], dT), 0.0f, t_max);
     S.ptemp[t] = tp;
     const float f = clampf_(__fdiv_rn(__fsub_rn(tp, t_sol), __fsub_rn(t_liq, t_sol)), 0.0f, 1.0f);

@@ -18,6 +18,7 @@ CHUNK = 1024
 HF_PLAN_STREAMING_CG = 1
 HF_PLAN_NO_TMA = 2
 HF_PLAN_LANES_SHIFT = 8
+HF_PLAN_RES_TILES_SHIFT = 12
 
 _P = C.c_void_p
 

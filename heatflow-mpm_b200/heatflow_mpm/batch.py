@@ -202,7 +202,7 @@ def autotune(batch: AirBatch, dt=2e-3, reps=3, candidates=None, cache=True):
         best = tuple(int(v) for v in table[key]["choice"])
         plan.plan.persistent_blocks, plan.plan.group_cells, plan.lanes = best
         return best, table[key]["timings"]
-    candidates = candidates or [(b * sms, g, l) for (g, l) in ((0, 1), (0, 2), (1, 4), (0, 4))
+    candidates = candidates or [(b * sms, g, l) for (g, l) in ((1, 1), (1, 2), (0, 1), (0, 2), (1, 4), (0, 4))
                                 for b in (2, 4, 5)]
     timings = {}
     for pb, gc, ln in candidates:

@@ -256,6 +256,17 @@ class ScenePlan:
             raise ValueError("lanes must be 0..8")
         self.plan.options = (self.plan.options & ~(15 << _lib.HF_PLAN_LANES_SHIFT)) | (int(k) << _lib.HF_PLAN_LANES_SHIFT)
 
+    @property
+    def resident_tiles(self):
+        """Tiles per 256-thread group of the single-scene resident CG variant (0: the fewest that fit)."""
+        return (self.plan.options >> _lib.HF_PLAN_RES_TILES_SHIFT) & 3
+
+    @resident_tiles.setter
+    def resident_tiles(self, m):
+        if not 0 <= int(m) <= 3:
+            raise ValueError("resident_tiles must be 0..3")
+        self.plan.options = (self.plan.options & ~(3 << _lib.HF_PLAN_RES_TILES_SHIFT)) | (int(m) << _lib.HF_PLAN_RES_TILES_SHIFT)
+
     def stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
 

@@ -115,6 +115,8 @@ typedef struct hf_scene {
 #define HF_PLAN_NO_TMA 2u            /* resident pressure CG without the TMA-staged stencil */
 #define HF_PLAN_LANES_SHIFT 8        /* options bits 8..11: lanes of the streaming CG launch (independent scene groups
                                         solved side by side, each lane with its own barrier; 0 = one lane) */
+#define HF_PLAN_RES_TILES_SHIFT 12   /* options bits 12..13: tiles per 256-thread group of the resident CG variant (1..3;
+                                        0 = the fewest that fit; more tiles per group = fewer threads, more registers) */
 
 /* A batch of scenes ready to launch: tables in device memory plus the host copy used to size launches. */
 typedef struct hf_plan {
