@@ -180,6 +180,10 @@ int hf_cell_velocity(const hf_plan *plan, int s, float *out, void *stream);
 /* grid.py:257-263: max|div(alpha_f u + q)| * h and max |u|,|v|,|w|; result written to out_dev[0] (float, device) */
 int hf_divergence_max(const hf_plan *plan, int s, float *out_dev, void *stream);
 int hf_speed_max(const hf_plan *plan, int s, float *out_dev, void *stream);
+/* solver.py:105-110 frame_dict as written by scripts/run_scene.py:31-40: grid_T (n^3), the cell-centred air velocity
+   (n^3 x 3, grid.py:156-162) and the particles' temperature and melt fraction (n_particles each) of scene `s`, converted
+   to binary16 (round to nearest even, as numpy's astype(float16)) into device buffers; any output may be NULL */
+int hf_pack_frame(const hf_plan *plan, int s, void *grid_T, void *air_u, void *temp, void *melt, void *stream);
 
 /* ------------------------------------------------------------- single-kernel entry points (parity, unit tests) */
 /* grid.py:94-115 k_laplacian: out = alpha * L(p) / h^2 + beta * y (n^3 arrays, one scene) */
