@@ -36,7 +36,7 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
 struct DeviceInfo {
     int sms = 0;
     int coop = 0;
-    int occ_heat = 0, occ_pressure = 0;
+    int occ_heat = 0, occ_pressure = 0, occ_pressure_tma = 0;
     size_t smem_optin = 0;
     bool ready = false;
     // occupancy of each resident variant [heat][tiles per group][tma][groups] (-1: not queried yet; the query also
@@ -61,8 +61,12 @@ int device_info(DeviceInfo** out) {
         if (major != 10) return fail(HF_ERR_DEVICE, "libheatflow_b200 is built for sm_100a (B200); this device is not sm_100");
         HF_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
         HF_CUDA(cudaDeviceGetAttribute(&d.coop, cudaDevAttrCooperativeLaunch, dev), "cudaDeviceGetAttribute");
-        HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_heat, hf::pcg_kernel(true), hf::kThreads, 0), "occupancy");
-        HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_pressure, hf::pcg_kernel(false), hf::kThreads, 0),
+        HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_heat, hf::pcg_kernel(true, false), hf::kThreads, 0),
+                "occupancy");
+        HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_pressure, hf::pcg_kernel(false, false), hf::kThreads, 0),
+                "occupancy");
+        HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_pressure_tma, hf::pcg_kernel(false, true), hf::kThreads,
+                                                              hf::pcg_stream_smem(true)),
                 "occupancy");
         int optin = 0;
         HF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "cudaDeviceGetAttribute");
@@ -81,7 +85,7 @@ constexpr size_t kHeadBytes = 256;           // barrier counters, group queue, l
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
-    size_t head, chunk_begin, tile_begin, ctl, partA, partB, mean_part, total;
+    size_t head, chunk_begin, tile_begin, maps, partA, partB, mean_part, total;
 };
 
 Layout layout(int S, int C, int T) {
@@ -93,8 +97,8 @@ Layout layout(int S, int C, int T) {
     o = align_up(o + sizeof(int) * (size_t)(S + 1), 256);
     L.tile_begin = o;
     o = align_up(o + sizeof(int) * (size_t)(S + 1), 256);
-    L.ctl = o;
-    o = align_up(o + sizeof(hf::CgCtl) * (size_t)S, 256);
+    L.maps = o;                      // 6 TMA descriptors per scene (128 bytes each)
+    o = align_up(o + sizeof(CUtensorMap) * 6 * (size_t)S, 256);
     L.partA = o;
     o = align_up(o + sizeof(double) * 3 * (size_t)T, 256);
     L.partB = o;
@@ -115,7 +119,7 @@ hf::Workspace workspace(const hf_plan* p) {
     w.err = w.lane_next + 2 * hf::kMaxLanes;
     w.chunk_begin = reinterpret_cast<int*>(b + L.chunk_begin);
     w.tile_begin = reinterpret_cast<int*>(b + L.tile_begin);
-    w.ctl = reinterpret_cast<hf::CgCtl*>(b + L.ctl);
+    w.maps = reinterpret_cast<const CUtensorMap*>(b + L.maps);
     w.partA = reinterpret_cast<double*>(b + L.partA);
     w.partB = reinterpret_cast<double*>(b + L.partB);
     w.mean_part = reinterpret_cast<double*>(b + L.mean_part);
@@ -143,6 +147,21 @@ int encode_map(CUtensorMap* m, const float* base, int nk, int nj, int ni, int bk
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(HF_ERR_DEVICE, "cuTensorMapEncodeTiled failed");
     return HF_OK;
+}
+
+// The six TMA descriptors of a scene's tiled pressure stencil (order of hf::TileMaps): z and both search-direction
+// buffers with a one-cell halo, alpha_f x on its face lattice, alpha_f y and z in cell layout.
+static_assert(sizeof(hf::TileMaps) == 6 * sizeof(CUtensorMap), "TileMaps is six consecutive descriptors");
+
+int encode_scene_maps(const hf_scene& sc, CUtensorMap* m) {
+    const int n = sc.n;
+    int rc;
+    if ((rc = encode_map(&m[0], sc.cg_z, n, n, n, 40, 10, 6))) return rc;
+    if ((rc = encode_map(&m[1], sc.cg_p[0], n, n, n, 40, 10, 6))) return rc;
+    if ((rc = encode_map(&m[2], sc.cg_p[1], n, n, n, 40, 10, 6))) return rc;
+    if ((rc = encode_map(&m[3], sc.ax, n, n, n + 1, 32, 8, 5))) return rc;
+    if ((rc = encode_map(&m[4], sc.ayc, n, n, n, 32, 9, 4))) return rc;
+    return encode_map(&m[5], sc.azc, n, n, n, 36, 8, 4);
 }
 
 int check_plan(const hf_plan* p) {
@@ -192,15 +211,7 @@ int launch_resident(const hf_plan* p, DeviceInfo* d, bool heat, double dt, int s
         if (occ < 1) continue;
         hf::TileMaps maps;
         std::memset(&maps, 0, sizeof maps);
-        if (tma) {
-            const int n = sc.n;
-            if ((rc = encode_map(&maps.z, sc.cg_z, n, n, n, 40, 10, 6))) return rc;
-            if ((rc = encode_map(&maps.p0, sc.cg_p[0], n, n, n, 40, 10, 6))) return rc;
-            if ((rc = encode_map(&maps.p1, sc.cg_p[1], n, n, n, 40, 10, 6))) return rc;
-            if ((rc = encode_map(&maps.ax, sc.ax, n, n, n + 1, 32, 8, 5))) return rc;
-            if ((rc = encode_map(&maps.ayc, sc.ayc, n, n, n, 32, 9, 4))) return rc;
-            if ((rc = encode_map(&maps.azc, sc.azc, n, n, n, 36, 8, 4))) return rc;
-        }
+        if (tma && (rc = encode_scene_maps(sc, &maps.z))) return rc;
         HF_CUDA(cudaMemsetAsync(ws.bar, 0, kHeadBytes, S(stream)), "cudaMemsetAsync(barrier)");
         void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&t_lo, (void*)&t_hi, (void*)&dt, (void*)&ws, (void*)&maps};
         HF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(256 * groups), args, smem, S(stream)),
@@ -226,7 +237,7 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
             total += tiles_of(p->scenes_host[s].n);
         }
     if (total != p->num_tiles) return fail(HF_ERR_ARG, "plan changed since hf_plan_upload");
-    if (nactive == 1 && !(p->options & HF_PLAN_STREAMING_CG)) {
+    if (nactive == 1 && !(p->options & HF_PLAN_STREAMING_CG) && !(heat && (p->options & HF_PLAN_STREAMING_HEAT))) {
         rc = launch_resident(p, d, heat, dt, last, stream);
         if (rc != -1) return rc;
     }
@@ -255,7 +266,16 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
         s_last = s;
         t += tiles_of(p->scenes_host[s].n);
     }
-    const int occ = heat ? d->occ_heat : d->occ_pressure;
+    // the pressure stencil from TMA-staged boxes when the plan's descriptors exist and every active scene has them
+    bool tma = !heat && (p->options & HF_PLAN_MAPS_READY) && !(p->options & HF_PLAN_NO_TMA);
+    for (int s = 0; tma && s < p->num_scenes; ++s) {
+        const hf_scene& sc = p->scenes_host[s];
+        // the same test as hf_plan_upload's: only then does the workspace hold this scene's descriptors
+        if ((sc.flags & HF_FLAG_ACTIVE) && (sc.n % 4 != 0 || !sc.cg_z || !sc.cg_p[0] || !sc.cg_p[1] || !sc.ax || !sc.ayc ||
+                                            !sc.azc))
+            tma = false;
+    }
+    const int occ = heat ? d->occ_heat : tma ? d->occ_pressure_tma : d->occ_pressure;
     if (occ <= 0) return fail(HF_ERR_DEVICE, "persistent CG kernel does not fit on an SM");
     int lanes = (int)((p->options >> HF_PLAN_LANES_SHIFT) & 15u);
     if (lanes <= 0) lanes = 1;
@@ -271,7 +291,8 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
     const hf::TileItem* tiles = static_cast<const hf::TileItem*>(p->tiles_dev);
     HF_CUDA(cudaMemsetAsync(ws.bar, 0, kHeadBytes, S(stream)), "cudaMemsetAsync(barrier)");
     void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&dt, (void*)&ws, (void*)&gt};
-    HF_CUDA(cudaLaunchCooperativeKernel(hf::pcg_kernel(heat), dim3(grid), dim3(hf::kThreads), args, 0, S(stream)),
+    HF_CUDA(cudaLaunchCooperativeKernel(hf::pcg_kernel(heat, tma), dim3(grid), dim3(hf::kThreads), args,
+                                        hf::pcg_stream_smem(tma), S(stream)),
             "cooperative launch (CG)");
     return HF_OK;
 }
@@ -348,7 +369,21 @@ int hf_plan_upload(hf_plan* p, void* stream) {
             "upload chunk offsets");
     HF_CUDA(cudaMemcpyAsync(b + L.tile_begin, tbegin.data(), sizeof(int) * tbegin.size(), cudaMemcpyHostToDevice, S(stream)),
             "upload tile offsets");
+    // TMA descriptors of every active scene whose stencil boxes fit the alignment rules (n % 4 == 0); zero otherwise
+    std::vector<CUtensorMap> maps(6 * (size_t)p->num_scenes);
+    std::memset(maps.data(), 0, sizeof(CUtensorMap) * maps.size());
+    for (int s = 0; s < p->num_scenes; ++s) {
+        const hf_scene& sc = p->scenes_host[s];
+        if (!(sc.flags & HF_FLAG_ACTIVE) || sc.n % 4 != 0 || !sc.cg_z || !sc.cg_p[0] || !sc.cg_p[1] || !sc.ax || !sc.ayc ||
+            !sc.azc)
+            continue;
+        int rc = encode_scene_maps(sc, &maps[6 * (size_t)s]);
+        if (rc) return rc;
+    }
+    HF_CUDA(cudaMemcpyAsync(b + L.maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, S(stream)),
+            "upload TMA descriptors");
     HF_CUDA(cudaStreamSynchronize(S(stream)), "cudaStreamSynchronize(plan upload)");
+    p->options |= HF_PLAN_MAPS_READY;
     return HF_OK;
 }
 

@@ -372,6 +372,48 @@ __device__ __forceinline__ void write_stats(const hf_scene& S, const LocalScene&
     }
 }
 
+// ============================================================================================ TMA staging
+// Box geometry of the tiled pressure stencil (elements, innermost k first), all at 16-byte aligned k origins:
+//   z / p_old : k in [k0-4, k0+36), j in [j0-1, j0+9), i in [i0-1, i0+5)   (one-cell halo; k widened to alignment)
+//   alpha_f x : k in [k0, k0+32),   j in [j0, j0+8),   i in [i0, i0+5)     (low faces of the tile + next i layer)
+//   alpha_f y : k in [k0, k0+32),   j in [j0, j0+9),   i in [i0, i0+4)
+//   alpha_f z : k in [k0, k0+36),   j in [j0, j0+8),   i in [i0, i0+4)
+// Out-of-range elements are zero-filled by the copy engine and never used (domain faces are skipped).
+constexpr int kBZ = 40 * 10 * 6, kBX = 32 * 8 * 5, kBY = 32 * 9 * 4, kBW = 36 * 8 * 4;
+constexpr int kSlotFloats = 2 * kBZ + kBX + kBY + kBW;   // 8384 floats = 33,536 bytes (a multiple of 128)
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// bounded wait for the given phase; returns false on timeout
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phase) {
+    const unsigned long long t0 = global_timer_ns();
+    for (unsigned spins = 0;; ++spins) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(smem_addr(bar)), "r"(phase)
+            : "memory");
+        if (ok) return true;
+        if ((spins & 63u) == 63u && global_timer_ns() - t0 > kBarrierTimeoutNs) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int x, int y, int z, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+
 // ================================================================================================== streaming
 // A launch solves the groups of a GroupTable: consecutive scenes whose CG vectors the host sized to stay in L2.  The
 // grid is split into gt.lanes lanes of equal size (lane = blockIdx.x / blocks per lane), each with its own barrier;
@@ -380,10 +422,11 @@ __device__ __forceinline__ void write_stats(const hf_scene& S, const LocalScene&
 // lane's blocks (an equal share of every live scene per block while scenes converge at different iterations); every
 // block sums the tile partials of every scene of the group itself (same bits everywhere) and keeps the scalars in
 // shared memory, so an iteration takes two lane barriers.  Returns false when a barrier timed out.
-template <bool HEAT>
+template <bool HEAT, bool TMA>
 __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, const int4 grp,
                             int lb, int nlb, unsigned* bar, unsigned& epoch, double dt_d, const Workspace& ws,
-                            double* red, LocalScene* loc, unsigned char* s_par, int* s_any) {
+                            double* red, LocalScene* loc, unsigned char* s_par, int* s_any, float* slot,
+                            unsigned long long* mb, unsigned& tphase) {
     const int scene_lo = grp.x, scene_hi = grp.y, tile_lo = grp.z, tile_hi = grp.w;
     const int ns = scene_hi - scene_lo;
     double* bufA = ws.partA;
@@ -470,6 +513,63 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             const hf_scene& S = scenes[ti.scene];
             const int n = S.n;
             const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
+            if constexpr (TMA) {
+                // stage z and p_{k-1} with a one-cell halo and the tile's face fractions (resident-kernel geometry),
+                // form p_k in place, A p from shared memory; the block's other tiles wait in other blocks' slots
+                const bool first_it = kit == 1;
+                if (lt == 0) {
+                    asm volatile("fence.proxy.async.global;" ::: "memory");
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    const bool go = *(volatile int*)ws.err == 0;
+                    const CUtensorMap* M = ws.maps + 6 * ti.scene;
+                    mbar_expect_tx(mb, go ? (unsigned)(((first_it ? 1 : 2) * kBZ + kBX + kBY + kBW) * sizeof(float)) : 0u);
+                    if (go) {
+                        tma_load_3d(slot, &M[0], ti.k0 - 4, ti.j0 - 1, ti.i0 - 1, mb);
+                        if (!first_it) tma_load_3d(slot + kBZ, &M[1 + ((kit - 1) & 1)], ti.k0 - 4, ti.j0 - 1, ti.i0 - 1, mb);
+                        tma_load_3d(slot + 2 * kBZ, &M[3], ti.k0, ti.j0, ti.i0, mb);
+                        tma_load_3d(slot + 2 * kBZ + kBX, &M[4], ti.k0, ti.j0, ti.i0, mb);
+                        tma_load_3d(slot + 2 * kBZ + kBX + kBY, &M[5], ti.k0, ti.j0, ti.i0, mb);
+                    }
+                }
+                if (!mbar_wait(mb, tphase)) {
+                    if (lt == 0) atomicExch(ws.err, 1);
+                    mbar_wait(mb, tphase);   // a copy still in flight lands before the slot is used again
+                }
+                tphase ^= 1u;
+                if (!first_it)
+                    for (int e = lt; e < kBZ; e += kThreads) slot[e] = __fadd_rn(slot[e], __fmul_rn(L.beta, slot[kBZ + e]));
+                __syncthreads();
+                const float* axb = slot + 2 * kBZ;
+                const float* ayb = axb + kBX;
+                const float* azb = ayb + kBY;
+                float* pnew = S.cg_p[kit & 1];
+                double part[1] = {0.0};
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const Cell cl = tile_cell(ti, n, lt, m);
+                    if (!cl.ok) continue;
+                    const int bi = m, bj = lt >> 5, bk = lt & 31;
+                    const int o = (bi + 1) * 400 + (bj + 1) * 40 + (bk + 4);
+                    const float pc = slot[o];
+                    float acc = 0.0f;
+                    if (cl.i > 0) acc = __fadd_rn(acc, __fmul_rn(axb[bi * 256 + bj * 32 + bk], __fsub_rn(pc, slot[o - 400])));
+                    if (cl.i < n - 1)
+                        acc = __fadd_rn(acc, __fmul_rn(axb[(bi + 1) * 256 + bj * 32 + bk], __fsub_rn(pc, slot[o + 400])));
+                    if (cl.j > 0) acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + bj * 32 + bk], __fsub_rn(pc, slot[o - 40])));
+                    if (cl.j < n - 1)
+                        acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + (bj + 1) * 32 + bk], __fsub_rn(pc, slot[o + 40])));
+                    if (cl.k > 0) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk], __fsub_rn(pc, slot[o - 1])));
+                    if (cl.k < n - 1)
+                        acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk + 1], __fsub_rn(pc, slot[o + 1])));
+                    const float ap = __fdiv_rn(acc, hh);
+                    pnew[cl.t] = pc;
+                    S.cg_Ap[cl.t] = ap;
+                    part[0] += (double)pc * (double)ap;
+                }
+                group_sum<1>(part, red);   // its __syncthreads also ends every read of the slot
+                if (lt == 0) bufA[3 * c] = part[0];
+                continue;
+            }
             const Dir P{S.cg_z, S.cg_p[(kit - 1) & 1], L.beta, kit == 1};
             float pc[4], ap[4];
 #pragma unroll
@@ -594,13 +694,22 @@ done:
     return ok;
 }
 
-template <bool HEAT>
+template <bool HEAT, bool TMA>
 __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles,
                                                  double dt_d, Workspace ws, const __grid_constant__ GroupTable gt) {
     __shared__ double red[kRedComps * 32];
     __shared__ LocalScene loc[kGroupScenes];
     __shared__ unsigned char s_par[kGroupScenes];
     __shared__ int s_any;
+    __shared__ __align__(8) unsigned long long mbar[1];
+    extern __shared__ __align__(128) float sm_raw[];
+    float* slot = TMA ? reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127) : nullptr;
+    unsigned tphase = 0;
+    if (TMA && threadIdx.x == 0) {
+        mbar_init(&mbar[0], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
     const int nlb = gridDim.x / gt.lanes;           // blocks per lane (the host launches a multiple of gt.lanes)
     const int lane = blockIdx.x / nlb, lb = blockIdx.x % nlb;
     unsigned* bar = ws.bar + (HEAT ? 0 : kMaxLanes) + lane;
@@ -612,7 +721,9 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
         if (!grid_barrier(bar, epoch, ws.err, nlb)) break;
         const int g = *(volatile int*)next;
         if (g >= gt.count) break;
-        if (!solve_group<HEAT>(scenes, tiles, gt.g[g], lb, nlb, bar, epoch, dt_d, ws, red, loc, s_par, &s_any)) break;
+        if (!solve_group<HEAT, TMA>(scenes, tiles, gt.g[g], lb, nlb, bar, epoch, dt_d, ws, red, loc, s_par, &s_any, slot,
+                                    &mbar[0], tphase))
+            break;
     }
     // a timed-out barrier leaves the groups that no lane reached unsolved: flag their scenes
     if (blockIdx.x == 0 && *(volatile int*)ws.err) {
@@ -620,48 +731,6 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
             for (int s = gt.g[q].x + (int)threadIdx.x; s < gt.g[q].y; s += kThreads)
                 if (scenes[s].flags & HF_FLAG_ACTIVE) scenes[s].state->status |= HF_SCENE_BARRIER_TIMEOUT;
     }
-}
-
-// ============================================================================================ TMA staging
-// Box geometry of the tiled pressure stencil (elements, innermost k first), all at 16-byte aligned k origins:
-//   z / p_old : k in [k0-4, k0+36), j in [j0-1, j0+9), i in [i0-1, i0+5)   (one-cell halo; k widened to alignment)
-//   alpha_f x : k in [k0, k0+32),   j in [j0, j0+8),   i in [i0, i0+5)     (low faces of the tile + next i layer)
-//   alpha_f y : k in [k0, k0+32),   j in [j0, j0+9),   i in [i0, i0+4)
-//   alpha_f z : k in [k0, k0+36),   j in [j0, j0+8),   i in [i0, i0+4)
-// Out-of-range elements are zero-filled by the copy engine and never used (domain faces are skipped).
-constexpr int kBZ = 40 * 10 * 6, kBX = 32 * 8 * 5, kBY = 32 * 9 * 4, kBW = 36 * 8 * 4;
-constexpr int kSlotFloats = 2 * kBZ + kBX + kBY + kBW;   // 8384 floats = 33,536 bytes (a multiple of 128)
-
-__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-
-// bounded wait for the given phase; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phase) {
-    const unsigned long long t0 = global_timer_ns();
-    for (unsigned spins = 0;; ++spins) {
-        unsigned ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(ok)
-            : "r"(smem_addr(bar)), "r"(phase)
-            : "memory");
-        if (ok) return true;
-        if ((spins & 63u) == 63u && global_timer_ns() - t0 > kBarrierTimeoutNs) return false;
-    }
-}
-
-__device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int x, int y, int z, unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-        ::"r"(smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
-        : "memory");
 }
 
 // ======================================================================================= register-resident
@@ -1242,7 +1311,11 @@ finish:
     if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, false, *(volatile int*)ws.err != 0, par);
 }
 
-const void* pcg_kernel(bool heat) { return heat ? (const void*)k_pcg<true> : (const void*)k_pcg<false>; }
+const void* pcg_kernel(bool heat, bool tma) {
+    return heat ? (const void*)k_pcg<true, false> : tma ? (const void*)k_pcg<false, true> : (const void*)k_pcg<false, false>;
+}
+
+size_t pcg_stream_smem(bool tma) { return tma ? (size_t)kSlotFloats * sizeof(float) + 128 : 0; }
 
 const void* pcg_resident_kernel(bool heat, int maxc, bool tma) {
     if (heat) {

@@ -7,14 +7,6 @@
 
 namespace hf {
 
-// Per-scene control block of a CG solve (and the pressure-rhs mean), written by the block that finalises a scene's
-// reduction and read by every block after the following grid barrier.
-struct CgCtl {
-    double bb, rr, rz, pAp, atol_sq, mean;
-    float alpha, beta;
-    int iters, live, status, maxit;
-};
-
 constexpr int kMaxLanes = 8;      // lanes of one streaming CG launch
 constexpr int kGroupScenes = 32;  // scenes of one CG group (every block of a lane keeps all their scalars)
 constexpr int kMaxGroups = 1024;  // groups of one launch (a kernel parameter: 16 KB)
@@ -33,7 +25,7 @@ struct Workspace {
     int* err;               // [1] barrier timeout flag
     int* chunk_begin;       // [S+1] first chunk of every scene in the chunk table
     int* tile_begin;        // [S+1] first tile of every scene in the tile table
-    CgCtl* ctl;             // [S] per-scene CG record written by the scene's owner block
+    const CUtensorMap* maps;  // [6 S] per scene: z, p_0, p_1, alpha_f x, alpha_f y (cells), alpha_f z (cells) boxes
     double* partA;          // [3*T] per-tile fp64 partials of CG phase A
     double* partB;          // [3*T] per-tile fp64 partials of the CG set-up and phase B
     double* mean_part;      // [C] per-chunk fp64 sums of the pressure rhs
@@ -64,9 +56,12 @@ __global__ void k_heat_matvec_plain(int n, float h, float dt, float alpha, float
                                     const float* __restrict__ kap, const uint8_t* __restrict__ fl,
                                     const float* __restrict__ y, float* __restrict__ out);
 // persistent cooperative Jacobi-PCG kernel over the groups of a GroupTable (heat = heat system, else pressure system +
-// projection + end of substep); arguments: (const hf_scene*, const TileItem*, double dt, Workspace, GroupTable); the
+// projection + end of substep; tma: pressure stencil staged by TMA from the workspace's descriptors, every scene of
+// the table with n % 4 == 0); arguments: (const hf_scene*, const TileItem*, double dt, Workspace, GroupTable); the
 // grid is a multiple of the table's lanes
-const void* pcg_kernel(bool heat);
+const void* pcg_kernel(bool heat, bool tma);
+// dynamic shared memory of the streaming kernel (tma: one stencil slot per block, staged with TMA)
+size_t pcg_stream_smem(bool tma);
 // register-resident single-scene variant (MAXC tiles per 256-thread group: 1, 2 or 3; blockDim = 256 x groups);
 // arguments: (const hf_scene*, const TileItem*, int tile_lo, int tile_hi, double dt, Workspace, TileMaps) -- the
 // scene's tiles; the TileMaps is used when tma; dynamic shared memory pcg_resident_smem(...)

@@ -17,6 +17,7 @@ HF_SCENE_HEAT_MAXITER, HF_SCENE_PRESSURE_MAXITER, HF_SCENE_NONFINITE, HF_SCENE_B
 CHUNK = 1024
 HF_PLAN_STREAMING_CG = 1
 HF_PLAN_NO_TMA = 2
+HF_PLAN_STREAMING_HEAT = 4
 HF_PLAN_LANES_SHIFT = 8
 HF_PLAN_RES_TILES_SHIFT = 12
 

@@ -113,6 +113,10 @@ typedef struct hf_scene {
 #define HF_PLAN_STREAMING_CG 1u      /* never use the register-resident CG variant (single-scene plans use it when
                                         the scene's tiles fit one block per SM) */
 #define HF_PLAN_NO_TMA 2u            /* resident pressure CG without the TMA-staged stencil */
+#define HF_PLAN_STREAMING_HEAT 4u    /* the heat CG of a single-scene plan in the streaming kernel (pressure unchanged) */
+#define HF_PLAN_MAPS_READY 0x8000u   /* set by hf_plan_upload: the workspace holds the scenes' TMA descriptors (the
+                                        streaming pressure CG stages its stencil boxes with TMA when every active scene
+                                        has n % 4 == 0) */
 #define HF_PLAN_LANES_SHIFT 8        /* options bits 8..11: lanes of the streaming CG launch (independent scene groups
                                         solved side by side, each lane with its own barrier; 0 = one lane) */
 #define HF_PLAN_RES_TILES_SHIFT 12   /* options bits 12..13: tiles per 256-thread group of the resident CG variant (1..3;
