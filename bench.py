@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="plain line without the batched/served summaries")
     ap.add_argument("--resident-tiles", type=int, default=0, help="plain: tiles per group of the resident CG (0: auto)")
     ap.add_argument("--no-graph", action="store_true", help="plain: time eager launches instead of one graph replay")
+    ap.add_argument("--streaming", default="none", choices=["none", "heat", "both"],
+                    help="plain: CG solves in the streaming kernel instead of the resident one")
+    ap.add_argument("--persistent-blocks", type=int, default=0, help="plain: grid of the streaming CG kernel")
     ap.add_argument("--scenes", type=int, default=64, help="batched: scenes in the ensemble")
     ap.add_argument("--graph-steps", type=int, default=10, help="batched: substeps per captured CUDA graph")
     ap.add_argument("--edges", default="32,48,64,96,128", help="batched: grid edges the ensemble draws from")
@@ -293,6 +296,9 @@ def bench_plain(args, dev, rank, world, local):
     sim = coupled_default(device=dev)
     sc, plan = sim.scene, sim.plan
     plan.resident_tiles = args.resident_tiles
+    plan.plan.persistent_blocks = args.persistent_blocks
+    from heatflow_mpm import _lib as L_
+    plan.plan.options |= {"none": 0, "heat": L_.HF_PLAN_STREAMING_HEAT, "both": L_.HF_PLAN_STREAMING_CG}[args.streaming]
     n = sim.grid.n
     N = n ** 3
     stream = torch.cuda.current_stream()
@@ -480,7 +486,7 @@ def bench_batched(args, dev, rank, world, local, steps, warmup, cpu_sample=True)
                    for s, a, b in zip(mine, sa, sbk))
     peaks = load_peaks()
     roof = roofline(cg_bytes / (cg_ms / 1000.0) / 1e9, peaks, traffic=None,
-                    kernel="k_pcg<0> (streaming persistent pressure Jacobi-PCG + projection over the scene table)",
+                    kernel="k_pcg<false, true> (streaming persistent pressure Jacobi-PCG + projection over the scene table, TMA-staged double-buffered tile boxes)",
                     bytes_per_launch=cg_bytes, ms_per_launch=cg_ms, measured_on="rank 0 stage breakdown, 10 substeps")
     sub_gbs = sb / (el_ms / steps / 1000.0) / 1e9
     # ---- end to end through the public API: AirBatch.substep per substep, every scene's status block read back

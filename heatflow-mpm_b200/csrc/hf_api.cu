@@ -65,6 +65,9 @@ int device_info(DeviceInfo** out) {
                 "occupancy");
         HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_pressure, hf::pcg_kernel(false, false), hf::kThreads, 0),
                 "occupancy");
+        HF_CUDA(cudaFuncSetAttribute(hf::pcg_kernel(false, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)hf::pcg_stream_smem(true)),
+                "smem attribute (streaming CG)");
         HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_pressure_tma, hf::pcg_kernel(false, true), hf::kThreads,
                                                               hf::pcg_stream_smem(true)),
                 "occupancy");
@@ -97,8 +100,8 @@ Layout layout(int S, int C, int T) {
     o = align_up(o + sizeof(int) * (size_t)(S + 1), 256);
     L.tile_begin = o;
     o = align_up(o + sizeof(int) * (size_t)(S + 1), 256);
-    L.maps = o;                      // 6 TMA descriptors per scene (128 bytes each)
-    o = align_up(o + sizeof(CUtensorMap) * 6 * (size_t)S, 256);
+    L.maps = o;                      // kMapsPerScene TMA descriptors per scene (128 bytes each)
+    o = align_up(o + sizeof(CUtensorMap) * hf::kMapsPerScene * (size_t)S, 256);
     L.partA = o;
     o = align_up(o + sizeof(double) * 3 * (size_t)T, 256);
     L.partB = o;
@@ -272,7 +275,7 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
         const hf_scene& sc = p->scenes_host[s];
         // the same test as hf_plan_upload's: only then does the workspace hold this scene's descriptors
         if ((sc.flags & HF_FLAG_ACTIVE) && (sc.n % 4 != 0 || !sc.cg_z || !sc.cg_p[0] || !sc.cg_p[1] || !sc.ax || !sc.ayc ||
-                                            !sc.azc))
+                                            !sc.azc || !sc.p || !sc.cg_r || !sc.cg_Ap || !sc.pdiag))
             tma = false;
     }
     const int occ = heat ? d->occ_heat : tma ? d->occ_pressure_tma : d->occ_pressure;
@@ -370,15 +373,20 @@ int hf_plan_upload(hf_plan* p, void* stream) {
     HF_CUDA(cudaMemcpyAsync(b + L.tile_begin, tbegin.data(), sizeof(int) * tbegin.size(), cudaMemcpyHostToDevice, S(stream)),
             "upload tile offsets");
     // TMA descriptors of every active scene whose stencil boxes fit the alignment rules (n % 4 == 0); zero otherwise
-    std::vector<CUtensorMap> maps(6 * (size_t)p->num_scenes);
+    std::vector<CUtensorMap> maps(hf::kMapsPerScene * (size_t)p->num_scenes);
     std::memset(maps.data(), 0, sizeof(CUtensorMap) * maps.size());
     for (int s = 0; s < p->num_scenes; ++s) {
         const hf_scene& sc = p->scenes_host[s];
         if (!(sc.flags & HF_FLAG_ACTIVE) || sc.n % 4 != 0 || !sc.cg_z || !sc.cg_p[0] || !sc.cg_p[1] || !sc.ax || !sc.ayc ||
-            !sc.azc)
+            !sc.azc || !sc.p || !sc.cg_r || !sc.cg_Ap || !sc.pdiag)
             continue;
-        int rc = encode_scene_maps(sc, &maps[6 * (size_t)s]);
+        CUtensorMap* m = &maps[hf::kMapsPerScene * (size_t)s];
+        int rc = encode_scene_maps(sc, m);
         if (rc) return rc;
+        // the CG vectors of the tile's own cells, one (32, 8, 4) box each: x (the pressure), p_0, p_1, r, Ap, D
+        const float* own[6] = {sc.p, sc.cg_p[0], sc.cg_p[1], sc.cg_r, sc.cg_Ap, sc.pdiag};
+        for (int q = 0; q < 6; ++q)
+            if ((rc = encode_map(&m[6 + q], own[q], sc.n, sc.n, sc.n, 32, 8, 4))) return rc;
     }
     HF_CUDA(cudaMemcpyAsync(b + L.maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, S(stream)),
             "upload TMA descriptors");

@@ -414,6 +414,34 @@ __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, 
         : "memory");
 }
 
+// Tiles c = first, first + step, ... < end of scenes still iterating, through two shared-memory slots: the boxes of the
+// next tile are requested (issue, thread 0) before the current tile is worked on, so the copy overlaps the work.
+// `work` must end with a __syncthreads after its last read of the slot (the slot is refilled next).  A wait that times
+// out sets the error flag and waits once more for the copy, so that no copy is left in flight.
+template <class Issue, class Work>
+__device__ __forceinline__ void pipelined_tiles(int first, int end, int step, const LocalScene* loc, int scene_lo,
+                                                const TileItem* __restrict__ tiles, float* slots,
+                                                unsigned long long* mbar, unsigned* ph, int* err, Issue issue, Work work) {
+    auto next_live = [&](int c) {
+        while (c < end && !loc[tiles[c].scene - scene_lo].live) c += step;
+        return c;
+    };
+    int cur = next_live(first), si = 0;
+    if (cur < end && threadIdx.x == 0) issue(cur, slots, &mbar[0]);
+    while (cur < end) {
+        const int nxt = next_live(cur + step);
+        if (nxt < end && threadIdx.x == 0) issue(nxt, slots + (si ^ 1) * kSlotFloats, &mbar[si ^ 1]);
+        if (!mbar_wait(&mbar[si], ph[si])) {
+            if (threadIdx.x == 0) atomicExch(err, 1);
+            mbar_wait(&mbar[si], ph[si]);
+        }
+        ph[si] ^= 1u;
+        work(cur, slots + si * kSlotFloats);
+        cur = nxt;
+        si ^= 1;
+    }
+}
+
 // ================================================================================================== streaming
 // A launch solves the groups of a GroupTable: consecutive scenes whose CG vectors the host sized to stay in L2.  The
 // grid is split into gt.lanes lanes of equal size (lane = blockIdx.x / blocks per lane), each with its own barrier;
@@ -425,8 +453,8 @@ __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, 
 template <bool HEAT, bool TMA>
 __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, const int4 grp,
                             int lb, int nlb, unsigned* bar, unsigned& epoch, double dt_d, const Workspace& ws,
-                            double* red, LocalScene* loc, unsigned char* s_par, int* s_any, float* slot,
-                            unsigned long long* mb, unsigned& tphase) {
+                            double* red, LocalScene* loc, unsigned char* s_par, int* s_any, float* slots,
+                            unsigned long long* mbar, unsigned* ph) {
     const int scene_lo = grp.x, scene_hi = grp.y, tile_lo = grp.z, tile_hi = grp.w;
     const int ns = scene_hi - scene_lo;
     double* bufA = ws.partA;
@@ -506,36 +534,31 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
     // ------------------------------------------------------------------------------------------ iterations
     for (int kit = 1; *s_any; ++kit) {
         // phase A: p_k at the stencil points, Ap = A p_k, p.Ap
-        for (int c = first; c < tile_hi; c += nlb) {
-            const TileItem ti = tiles[c];
-            const LocalScene& L = loc[ti.scene - scene_lo];
-            if (!L.live) continue;
-            const hf_scene& S = scenes[ti.scene];
-            const int n = S.n;
-            const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
-            if constexpr (TMA) {
-                // stage z and p_{k-1} with a one-cell halo and the tile's face fractions (resident-kernel geometry),
-                // form p_k in place, A p from shared memory; the block's other tiles wait in other blocks' slots
-                const bool first_it = kit == 1;
-                if (lt == 0) {
-                    asm volatile("fence.proxy.async.global;" ::: "memory");
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    const bool go = *(volatile int*)ws.err == 0;
-                    const CUtensorMap* M = ws.maps + 6 * ti.scene;
-                    mbar_expect_tx(mb, go ? (unsigned)(((first_it ? 1 : 2) * kBZ + kBX + kBY + kBW) * sizeof(float)) : 0u);
-                    if (go) {
-                        tma_load_3d(slot, &M[0], ti.k0 - 4, ti.j0 - 1, ti.i0 - 1, mb);
-                        if (!first_it) tma_load_3d(slot + kBZ, &M[1 + ((kit - 1) & 1)], ti.k0 - 4, ti.j0 - 1, ti.i0 - 1, mb);
-                        tma_load_3d(slot + 2 * kBZ, &M[3], ti.k0, ti.j0, ti.i0, mb);
-                        tma_load_3d(slot + 2 * kBZ + kBX, &M[4], ti.k0, ti.j0, ti.i0, mb);
-                        tma_load_3d(slot + 2 * kBZ + kBX + kBY, &M[5], ti.k0, ti.j0, ti.i0, mb);
-                    }
+        if constexpr (TMA) {
+            // stage z and p_{k-1} with a one-cell halo and the tile's face fractions (the resident kernel's box
+            // geometry), form p_k in place, A p from shared memory
+            const bool first_it = kit == 1;
+            auto issue = [&](int c, float* slot, unsigned long long* mb) {
+                const TileItem ti = tiles[c];
+                asm volatile("fence.proxy.async.global;" ::: "memory");
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const bool go = *(volatile int*)ws.err == 0;
+                const CUtensorMap* M = ws.maps + kMapsPerScene * ti.scene;
+                mbar_expect_tx(mb, go ? (unsigned)(((first_it ? 1 : 2) * kBZ + kBX + kBY + kBW) * sizeof(float)) : 0u);
+                if (go) {
+                    tma_load_3d(slot, &M[0], ti.k0 - 4, ti.j0 - 1, ti.i0 - 1, mb);
+                    if (!first_it) tma_load_3d(slot + kBZ, &M[1 + ((kit - 1) & 1)], ti.k0 - 4, ti.j0 - 1, ti.i0 - 1, mb);
+                    tma_load_3d(slot + 2 * kBZ, &M[3], ti.k0, ti.j0, ti.i0, mb);
+                    tma_load_3d(slot + 2 * kBZ + kBX, &M[4], ti.k0, ti.j0, ti.i0, mb);
+                    tma_load_3d(slot + 2 * kBZ + kBX + kBY, &M[5], ti.k0, ti.j0, ti.i0, mb);
                 }
-                if (!mbar_wait(mb, tphase)) {
-                    if (lt == 0) atomicExch(ws.err, 1);
-                    mbar_wait(mb, tphase);   // a copy still in flight lands before the slot is used again
-                }
-                tphase ^= 1u;
+            };
+            auto work = [&](int c, float* slot) {
+                const TileItem ti = tiles[c];
+                const LocalScene& L = loc[ti.scene - scene_lo];
+                const hf_scene& S = scenes[ti.scene];
+                const int n = S.n;
+                const float h = (float)S.h, hh = __fmul_rn(h, h);
                 if (!first_it)
                     for (int e = lt; e < kBZ; e += kThreads) slot[e] = __fadd_rn(slot[e], __fmul_rn(L.beta, slot[kBZ + e]));
                 __syncthreads();
@@ -568,8 +591,16 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
                 }
                 group_sum<1>(part, red);   // its __syncthreads also ends every read of the slot
                 if (lt == 0) bufA[3 * c] = part[0];
-                continue;
-            }
+            };
+            pipelined_tiles(first, tile_hi, nlb, loc, scene_lo, tiles, slots, mbar, ph, ws.err, issue, work);
+        }
+        for (int c = first; !TMA && c < tile_hi; c += nlb) {
+            const TileItem ti = tiles[c];
+            const LocalScene& L = loc[ti.scene - scene_lo];
+            if (!L.live) continue;
+            const hf_scene& S = scenes[ti.scene];
+            const int n = S.n;
+            const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
             const Dir P{S.cg_z, S.cg_p[(kit - 1) & 1], L.beta, kit == 1};
             float pc[4], ap[4];
 #pragma unroll
@@ -613,7 +644,53 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
         }
         __syncthreads();
         // phase B: x += alpha p, r -= alpha Ap, z = D r, r.r and r.z
-        for (int c = first; c < tile_hi; c += nlb) {
+        if constexpr (TMA) {
+            // the tile's x, p_k, r, Ap and D as five (32, 8, 4) boxes: element (m, lt / 32, lt % 32) at m 256 + lt
+            auto issue = [&](int c, float* slot, unsigned long long* mb) {
+                const TileItem ti = tiles[c];
+                asm volatile("fence.proxy.async.global;" ::: "memory");
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const bool go = *(volatile int*)ws.err == 0;
+                const CUtensorMap* M = ws.maps + kMapsPerScene * ti.scene;
+                mbar_expect_tx(mb, go ? (unsigned)(5 * 1024 * sizeof(float)) : 0u);
+                if (go) {
+                    tma_load_3d(slot, &M[6], ti.k0, ti.j0, ti.i0, mb);
+                    tma_load_3d(slot + 1024, &M[7 + (kit & 1)], ti.k0, ti.j0, ti.i0, mb);
+                    tma_load_3d(slot + 2048, &M[9], ti.k0, ti.j0, ti.i0, mb);
+                    tma_load_3d(slot + 3072, &M[10], ti.k0, ti.j0, ti.i0, mb);
+                    tma_load_3d(slot + 4096, &M[11], ti.k0, ti.j0, ti.i0, mb);
+                }
+            };
+            auto work = [&](int c, float* slot) {
+                const TileItem ti = tiles[c];
+                const LocalScene& L = loc[ti.scene - scene_lo];
+                const hf_scene& S = scenes[ti.scene];
+                const int n = S.n;
+                const float alpha = L.alpha;
+                double part[2] = {0.0, 0.0};
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const Cell cl = tile_cell(ti, n, lt, m);
+                    if (!cl.ok) continue;
+                    const int e = m * 256 + lt;
+                    const float xv = __fadd_rn(slot[e], __fmul_rn(alpha, slot[1024 + e]));
+                    const float rv = __fsub_rn(slot[2048 + e], __fmul_rn(alpha, slot[3072 + e]));
+                    const float zv = __fmul_rn(slot[4096 + e], rv);
+                    S.p[cl.t] = xv;
+                    S.cg_r[cl.t] = rv;
+                    S.cg_z[cl.t] = zv;
+                    part[0] += (double)rv * (double)rv;
+                    part[1] += (double)rv * (double)zv;
+                }
+                group_sum<2>(part, red);
+                if (lt == 0) {
+                    bufB[3 * c + 1] = part[0];
+                    bufB[3 * c + 2] = part[1];
+                }
+            };
+            pipelined_tiles(first, tile_hi, nlb, loc, scene_lo, tiles, slots, mbar, ph, ws.err, issue, work);
+        }
+        for (int c = first; !TMA && c < tile_hi; c += nlb) {
             const TileItem ti = tiles[c];
             const LocalScene& L = loc[ti.scene - scene_lo];
             if (!L.live) continue;
@@ -624,14 +701,16 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             const float* pk = S.cg_p[kit & 1];
             const float alpha = L.alpha;
             float xv[4], rv[4], zv[4];
+            {
 #pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                const Cell cl = tile_cell(ti, n, lt, m);
-                xv[m] = rv[m] = zv[m] = 0.0f;
-                if (!cl.ok) continue;
-                xv[m] = __fadd_rn(x[cl.t], __fmul_rn(alpha, pk[cl.t]));
-                rv[m] = __fsub_rn(S.cg_r[cl.t], __fmul_rn(alpha, S.cg_Ap[cl.t]));
-                zv[m] = __fmul_rn(D[cl.t], rv[m]);
+                for (int m = 0; m < 4; ++m) {
+                    const Cell cl = tile_cell(ti, n, lt, m);
+                    xv[m] = rv[m] = zv[m] = 0.0f;
+                    if (!cl.ok) continue;
+                    xv[m] = __fadd_rn(x[cl.t], __fmul_rn(alpha, pk[cl.t]));
+                    rv[m] = __fsub_rn(S.cg_r[cl.t], __fmul_rn(alpha, S.cg_Ap[cl.t]));
+                    zv[m] = __fmul_rn(D[cl.t], rv[m]);
+                }
             }
             double part[2] = {0.0, 0.0};
 #pragma unroll
@@ -701,12 +780,13 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
     __shared__ LocalScene loc[kGroupScenes];
     __shared__ unsigned char s_par[kGroupScenes];
     __shared__ int s_any;
-    __shared__ __align__(8) unsigned long long mbar[1];
+    __shared__ __align__(8) unsigned long long mbar[2];
     extern __shared__ __align__(128) float sm_raw[];
-    float* slot = TMA ? reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127) : nullptr;
-    unsigned tphase = 0;
+    float* slots = TMA ? reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127) : nullptr;
+    unsigned ph[2] = {0u, 0u};
     if (TMA && threadIdx.x == 0) {
         mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -721,8 +801,8 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
         if (!grid_barrier(bar, epoch, ws.err, nlb)) break;
         const int g = *(volatile int*)next;
         if (g >= gt.count) break;
-        if (!solve_group<HEAT, TMA>(scenes, tiles, gt.g[g], lb, nlb, bar, epoch, dt_d, ws, red, loc, s_par, &s_any, slot,
-                                    &mbar[0], tphase))
+        if (!solve_group<HEAT, TMA>(scenes, tiles, gt.g[g], lb, nlb, bar, epoch, dt_d, ws, red, loc, s_par, &s_any, slots,
+                                    mbar, ph))
             break;
     }
     // a timed-out barrier leaves the groups that no lane reached unsolved: flag their scenes
@@ -1315,7 +1395,7 @@ const void* pcg_kernel(bool heat, bool tma) {
     return heat ? (const void*)k_pcg<true, false> : tma ? (const void*)k_pcg<false, true> : (const void*)k_pcg<false, false>;
 }
 
-size_t pcg_stream_smem(bool tma) { return tma ? (size_t)kSlotFloats * sizeof(float) + 128 : 0; }
+size_t pcg_stream_smem(bool tma) { return tma ? 2 * (size_t)kSlotFloats * sizeof(float) + 128 : 0; }
 
 const void* pcg_resident_kernel(bool heat, int maxc, bool tma) {
     if (heat) {

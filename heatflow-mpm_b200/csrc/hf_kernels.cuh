@@ -10,6 +10,7 @@ namespace hf {
 constexpr int kMaxLanes = 8;      // lanes of one streaming CG launch
 constexpr int kGroupScenes = 32;  // scenes of one CG group (every block of a lane keeps all their scalars)
 constexpr int kMaxGroups = 1024;  // groups of one launch (a kernel parameter: 16 KB)
+constexpr int kMapsPerScene = 12; // TMA descriptors per scene in the workspace
 
 // Scene groups of a streaming CG launch: group q = scenes [g[q].x, g[q].y), tiles [g[q].z, g[q].w).
 struct GroupTable {
@@ -25,7 +26,8 @@ struct Workspace {
     int* err;               // [1] barrier timeout flag
     int* chunk_begin;       // [S+1] first chunk of every scene in the chunk table
     int* tile_begin;        // [S+1] first tile of every scene in the tile table
-    const CUtensorMap* maps;  // [6 S] per scene: z, p_0, p_1, alpha_f x, alpha_f y (cells), alpha_f z (cells) boxes
+    const CUtensorMap* maps;  // [kMapsPerScene S] per scene: the stencil boxes z, p_0, p_1, alpha_f x, alpha_f y (cells),
+                              // alpha_f z (cells); then tile boxes of x (p), p_0, p_1, r, Ap, D
     double* partA;          // [3*T] per-tile fp64 partials of CG phase A
     double* partB;          // [3*T] per-tile fp64 partials of the CG set-up and phase B
     double* mean_part;      // [C] per-chunk fp64 sums of the pressure rhs
