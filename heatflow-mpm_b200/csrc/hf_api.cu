@@ -233,14 +233,17 @@ int launch_pcg(const hf_plan* p, bool heat, double dt, void* stream) {
     if (rc) return rc;
     if (p->num_tiles == 0) return HF_OK;
     int nactive = 0, last = -1, total = 0;
+    bool correction = false;   // the outer defect correction runs in the streaming kernel only
     for (int s = 0; s < p->num_scenes; ++s)
         if (p->scenes_host[s].flags & HF_FLAG_ACTIVE) {
             ++nactive;
             last = s;
             total += tiles_of(p->scenes_host[s].n);
+            correction = correction || (p->scenes_host[s].flags & HF_FLAG_DEFECT_CORRECTION);
         }
     if (total != p->num_tiles) return fail(HF_ERR_ARG, "plan changed since hf_plan_upload");
-    if (nactive == 1 && !(p->options & HF_PLAN_STREAMING_CG) && !(heat && (p->options & HF_PLAN_STREAMING_HEAT))) {
+    if (nactive == 1 && !correction && !(p->options & HF_PLAN_STREAMING_CG) &&
+        !(heat && (p->options & HF_PLAN_STREAMING_HEAT))) {
         rc = launch_resident(p, d, heat, dt, last, stream);
         if (rc != -1) return rc;
     }

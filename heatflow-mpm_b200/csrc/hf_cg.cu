@@ -36,6 +36,7 @@ constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;   // 2 s
 // Components one group_sum / scene_sums call reduces at most: 3 inner products per tile x 3 tiles of a 256-thread
 // group (the resident variants' set-up).  Every CG kernel's `red` holds kRedComps x 32 doubles (one per warp).
 constexpr int kRedComps = 9;
+constexpr int kMaxCorrections = 2;   // restarts of one solve by the outer defect correction
 
 __device__ __forceinline__ int uidx_(int n, int i, int j, int k) { return (i * n + j) * n + k; }
 __device__ __forceinline__ int vidx_(int n, int i, int j, int k) { return (i * (n + 1) + j) * n + k; }
@@ -311,8 +312,12 @@ __device__ __forceinline__ void project_cell(const hf_scene& S, float* u, float*
 // Per-block copy of a scene's CG scalars; every block derives them from the same partial sums, so all copies agree.
 struct LocalScene {
     double rz, atol_sq, bb, rr, pAp, mean;
+    double true_rr;             // fp64 |b - A x|^2 of the outer defect correction (-1: not formed)
     float alpha, beta;
     int live, iters, maxit, status;
+    int kbase;                  // iterations before the last restart by the defect correction
+    int corrections;            // restarts so far
+    int dc;                     // the true residual is still to be checked (HF_FLAG_DEFECT_CORRECTION)
 };
 
 __device__ __forceinline__ void init_scalars(LocalScene& L, const hf_scene& S, bool heat, const double (&tot)[3], int N) {
@@ -332,6 +337,10 @@ __device__ __forceinline__ void init_scalars(LocalScene& L, const hf_scene& S, b
     L.alpha = 0.0f;
     L.status = isfinite(tot[1]) ? 0 : HF_SCENE_NONFINITE;
     L.live = tot[1] > L.atol_sq && isfinite(tot[1]) && L.maxit > 0;
+    L.true_rr = -1.0;
+    L.kbase = 0;
+    L.corrections = 0;
+    L.dc = (S.flags & HF_FLAG_DEFECT_CORRECTION) != 0;
 }
 
 // convergence test after phase B of iteration kit (warp: kernel_2 then the residual test)
@@ -348,6 +357,42 @@ __device__ __forceinline__ bool update_scalars(LocalScene& L, bool heat, double 
     return live;
 }
 
+// True residual b - A x of one cell for the outer defect correction: the binary32 operator (grid.py:94-115 with the
+// binary32 h^2; heat.py:94-105 with the binary32 dt/h^2 and face diffusivities) applied with every product and sum in
+// fp64 to the binary32 vectors.
+__device__ double true_residual_pressure(const hf_scene& S, const float* __restrict__ x, int t, int i, int j, int k,
+                                         double hh) {
+    const int n = S.n, nn = n * n;
+    const double xc = x[t];
+    double acc = 0.0;
+    if (i > 0) acc += (double)S.ax[uidx_(n, i, j, k)] * (xc - (double)x[t - nn]);
+    if (i < n - 1) acc += (double)S.ax[uidx_(n, i + 1, j, k)] * (xc - (double)x[t + nn]);
+    if (j > 0) acc += (double)S.ay[vidx_(n, i, j, k)] * (xc - (double)x[t - n]);
+    if (j < n - 1) acc += (double)S.ay[vidx_(n, i, j + 1, k)] * (xc - (double)x[t + n]);
+    if (k > 0) acc += (double)S.az[widx_(n, i, j, k)] * (xc - (double)x[t - 1]);
+    if (k < n - 1) acc += (double)S.az[widx_(n, i, j, k + 1)] * (xc - (double)x[t + 1]);
+    return (double)S.rhs[t] - acc / hh;
+}
+
+__device__ double true_residual_heat(const hf_scene& S, const float* __restrict__ x, int t, int i, int j, int k,
+                                     double c_dt) {
+    const int n = S.n, nn = n * n;
+    const double xc = x[t], b = S.hrhs[t];
+    if (S.cell_flags[t] & 1) return b - xc;
+    const int nbr[6] = {t - nn, t + nn, t - n, t + n, t - 1, t + 1};
+    const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
+    const int fidx[6] = {uidx_(n, i, j, k), uidx_(n, i + 1, j, k), vidx_(n, i, j, k), vidx_(n, i, j + 1, k),
+                         widx_(n, i, j, k), widx_(n, i, j, k + 1)};
+    const float* hk[3] = {S.hkx, S.hky, S.hkz};
+    double acc = 0.0;
+    for (int q = 0; q < 6; ++q) {
+        if (!in[q]) continue;
+        const double kf = hk[q >> 1][fidx[q]];
+        acc += (S.cell_flags[nbr[q]] & 1) ? kf * xc : kf * (xc - (double)x[nbr[q]]);
+    }
+    return b - (xc + c_dt * acc);
+}
+
 __device__ __forceinline__ void write_stats(const hf_scene& S, const LocalScene& L, bool heat, bool timed_out, int par) {
     hf_scene_state* st = S.state;
     if (heat) {
@@ -356,6 +401,7 @@ __device__ __forceinline__ void write_stats(const hf_scene& S, const LocalScene&
         st->heat_rr = L.rr;
         st->heat_atol = sqrt(L.atol_sq);
         st->heat_bb = L.bb;
+        st->heat_true_rr = L.true_rr;
         st->total_heat_iters += L.iters;
     } else {
         st->status |= L.status | (timed_out ? HF_SCENE_BARRIER_TIMEOUT : 0);
@@ -363,6 +409,7 @@ __device__ __forceinline__ void write_stats(const hf_scene& S, const LocalScene&
         st->pressure_rr = L.rr;
         st->pressure_atol = sqrt(L.atol_sq);
         st->pressure_bb = L.bb;
+        st->pressure_true_rr = L.true_rr;
         st->rhs_mean = L.mean;
         st->total_pressure_iters += L.iters;
         if (!timed_out) {
@@ -532,6 +579,9 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
     __syncthreads();
 
     // ------------------------------------------------------------------------------------------ iterations
+    // Rounds: CG iterations until every scene has stopped; then, for scenes with the outer defect correction, the true
+    // residual, and another round for the scenes it restarted.
+    for (;;) {
     for (int kit = 1; *s_any; ++kit) {
         // phase A: p_k at the stencil points, Ap = A p_k, p.Ap
         if constexpr (TMA) {
@@ -736,7 +786,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             double tot[2];
             const int comp[2] = {1, 2};
             scene_sums<2>(bufB, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
-            if (threadIdx.x == 0) update_scalars(loc[q], HEAT, tot[0], tot[1], kit);
+            if (threadIdx.x == 0) update_scalars(loc[q], HEAT, tot[0], tot[1], loc[q].kbase + kit);
         }
         if (threadIdx.x == 0) {
             int any = 0;
@@ -745,6 +795,112 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
         }
         __syncthreads();
     }
+    // ------------------------------------------------------------- outer defect correction (fp64 true residual)
+    if (threadIdx.x == 0) {
+        int any = 0;
+        for (int q = 0; q < ns; ++q) any |= loc[q].dc;
+        *s_any = any;
+    }
+    __syncthreads();
+    if (!*s_any) break;
+    // pass 1: r_true = b - A x in fp64 for the scenes to check, rounded into the Ap vector (free between solves)
+    for (int c = first; c < tile_hi; c += nlb) {
+        const TileItem ti = tiles[c];
+        if (!loc[ti.scene - scene_lo].dc) continue;
+        const hf_scene& S = scenes[ti.scene];
+        const int n = S.n, par = s_par[ti.scene - scene_lo];
+        const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn(dt, hh);
+        const float* x = HEAT ? S.T[par ^ 1] : S.p;
+        double part[1] = {0.0};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const Cell cl = tile_cell(ti, n, lt, m);
+            if (!cl.ok) continue;
+            const double rt = HEAT ? true_residual_heat(S, x, cl.t, cl.i, cl.j, cl.k, (double)c_dt)
+                                   : true_residual_pressure(S, x, cl.t, cl.i, cl.j, cl.k, (double)hh);
+            S.cg_Ap[cl.t] = __double2float_rn(rt);
+            part[0] += rt * rt;
+        }
+        group_sum<1>(part, red);
+        if (lt == 0) bufA[3 * c + 1] = part[0];
+    }
+    if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
+    for (int q = 0; q < ns; ++q) {
+        if (!loc[q].dc) continue;   // uniform: shared value
+        const int s = scene_lo + q;
+        double tot[1];
+        const int comp[1] = {1};
+        scene_sums<1>(bufA, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
+        if (threadIdx.x == 0) {
+            LocalScene& L = loc[q];
+            L.true_rr = tot[0];
+            // restart from x with the true residual when it is above the tolerance, the recurrence had converged
+            // (not stopped at maxiter or on a non-finite value) and corrections are left
+            const bool stopped = L.status & (HF_SCENE_NONFINITE | HF_SCENE_HEAT_MAXITER | HF_SCENE_PRESSURE_MAXITER);
+            L.live = isfinite(tot[0]) && tot[0] > L.atol_sq && !stopped && L.corrections < kMaxCorrections &&
+                     L.iters < L.maxit;
+            L.dc = L.live;
+            if (L.live) {
+                L.corrections += 1;
+                L.status |= HF_SCENE_CORRECTED;
+                L.kbase = L.iters;
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        int any = 0;
+        for (int q = 0; q < ns; ++q) any |= loc[q].live;
+        *s_any = any;
+    }
+    __syncthreads();
+    if (!*s_any) break;
+    // pass 2: r = r_true, z = D r for the restarted scenes; r.r and r.z start the next round (p_1 = z)
+    for (int c = first; c < tile_hi; c += nlb) {
+        const TileItem ti = tiles[c];
+        if (!loc[ti.scene - scene_lo].live) continue;
+        const hf_scene& S = scenes[ti.scene];
+        const int n = S.n;
+        const float* D = HEAT ? S.hdiag : S.pdiag;
+        double part[2] = {0.0, 0.0};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const Cell cl = tile_cell(ti, n, lt, m);
+            if (!cl.ok) continue;
+            const float r = S.cg_Ap[cl.t];
+            const float z = __fmul_rn(D[cl.t], r);
+            S.cg_r[cl.t] = r;
+            S.cg_z[cl.t] = z;
+            part[0] += (double)r * (double)r;
+            part[1] += (double)r * (double)z;
+        }
+        group_sum<2>(part, red);
+        if (lt == 0) {
+            bufB[3 * c + 1] = part[0];
+            bufB[3 * c + 2] = part[1];
+        }
+    }
+    if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
+    for (int q = 0; q < ns; ++q) {
+        if (!loc[q].live) continue;
+        const int s = scene_lo + q;
+        double tot[2];
+        const int comp[2] = {1, 2};
+        scene_sums<2>(bufB, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
+        if (threadIdx.x == 0) {
+            LocalScene& L = loc[q];
+            L.rr = tot[0];
+            L.rz = tot[1];
+            L.beta = 0.0f;
+            L.live = isfinite(tot[0]) && tot[0] > L.atol_sq;
+        }
+    }
+    if (threadIdx.x == 0) {
+        int any = 0;
+        for (int q = 0; q < ns; ++q) any |= loc[q].live;
+        *s_any = any;
+    }
+    __syncthreads();
+    }   // rounds
     // -------------------------------------------------------------------- pressure epilogue: projection
     if (!HEAT) {
         for (int c = first; c < tile_hi; c += nlb) {

@@ -12,7 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libheatflow_b200.so")
 
 HF_OK, HF_ERR_ARG, HF_ERR_CUDA, HF_ERR_WORKSPACE, HF_ERR_DEVICE = 0, 1, 2, 3, 4
-HF_FLAG_BUOYANCY, HF_FLAG_SOURCE, HF_FLAG_PARTICLES, HF_FLAG_ACTIVE = 1, 2, 4, 8
+HF_FLAG_BUOYANCY, HF_FLAG_SOURCE, HF_FLAG_PARTICLES, HF_FLAG_ACTIVE, HF_FLAG_DEFECT_CORRECTION = 1, 2, 4, 8, 16
+HF_SCENE_CORRECTED = 16
 HF_SCENE_HEAT_MAXITER, HF_SCENE_PRESSURE_MAXITER, HF_SCENE_NONFINITE, HF_SCENE_BARRIER_TIMEOUT = 1, 2, 4, 8
 CHUNK = 1024
 HF_PLAN_STREAMING_CG = 1
@@ -30,7 +31,8 @@ class SceneState(C.Structure):
                 ("heat_rr", C.c_double), ("heat_atol", C.c_double), ("pressure_rr", C.c_double),
                 ("pressure_atol", C.c_double), ("pressure_bb", C.c_double), ("heat_bb", C.c_double),
                 ("rhs_mean", C.c_double), ("total_heat_iters", C.c_int64), ("total_pressure_iters", C.c_int64),
-                ("box", C.c_int32 * 6), ("box_prev", C.c_int32 * 6), ("reserved_box", C.c_int32 * 4)]
+                ("box", C.c_int32 * 6), ("box_prev", C.c_int32 * 6), ("heat_true_rr", C.c_double),
+                ("pressure_true_rr", C.c_double)]
 
 
 SCENE_DOUBLES = ("h", "rho", "t_amb", "alpha_f_min", "g", "cg_tol", "heat_tol", "kappa_air", "kappa_mat", "rate",

@@ -59,6 +59,7 @@ class SceneSpec:
     mu_l: float = 30.0
     t_max: float = 300.0
     t_init_grid: float | None = None         # initial grid temperature (default t_amb)
+    defect_correction: bool = False          # fp64 true-residual check and restart after each CG solve (not in the reference)
     extra: dict = field(default_factory=dict)
 
 
@@ -166,6 +167,8 @@ class DeviceScene:
             flags |= _lib.HF_FLAG_SOURCE
         if sp.n_particles > 0:
             flags |= _lib.HF_FLAG_PARTICLES
+        if sp.defect_correction:
+            flags |= _lib.HF_FLAG_DEFECT_CORRECTION
         r.flags = flags
         r.cg_max_iter, r.heat_maxiter = sp.cg_max_iter, sp.heat_maxiter
         vals = dict(h=sp.h, rho=sp.rho, t_amb=sp.t_amb, alpha_f_min=sp.alpha_f_min, g=sp.g, cg_tol=sp.cg_tol,

@@ -41,12 +41,16 @@ typedef enum hf_status {
 #define HF_SCENE_PRESSURE_MAXITER 2  /* pressure CG stopped at maxiter above its tolerance */
 #define HF_SCENE_NONFINITE 4         /* a CG residual became NaN/inf */
 #define HF_SCENE_BARRIER_TIMEOUT 8   /* a grid barrier of a persistent kernel gave up (bounded wait) */
+#define HF_SCENE_CORRECTED 16        /* a CG solve was restarted by the outer defect correction (HF_FLAG_DEFECT_CORRECTION) */
 
 /* hf_scene.flags */
 #define HF_FLAG_BUOYANCY 1u          /* GridConfig.buoyancy (grid.py:18) */
 #define HF_FLAG_SOURCE 2u            /* heater source active: rate > 0 (solver.py:76) */
 #define HF_FLAG_PARTICLES 4u         /* particle coupling on: obstacle fields rebuilt every substep (solver.py:65-72) */
 #define HF_FLAG_ACTIVE 8u            /* scene takes part in batched calls (serving slots) */
+#define HF_FLAG_DEFECT_CORRECTION 16u /* after each CG solve converges, form the true residual b - A x in fp64; above the
+                                         tolerance, restart CG from x with it (at most twice).  Not in the reference:
+                                         off by default; the solves run in the streaming CG kernel */
 
 /* Mutable device-side state of one scene (caller allocates sizeof(hf_scene_state) bytes of device memory, zeroed). */
 typedef struct hf_scene_state {
@@ -65,7 +69,9 @@ typedef struct hf_scene_state {
      * (lo = INT32_MAX, hi = INT32_MIN) before the first substep. */
     int32_t box[6];
     int32_t box_prev[6];
-    int32_t reserved_box[4];
+    /* fp64 norm^2 of the true residual b - A x at the end of the last heat / pressure solve (scenes with
+       HF_FLAG_DEFECT_CORRECTION; -1 otherwise) */
+    double heat_true_rr, pressure_true_rr;
 } hf_scene_state;
 
 /* One scene: sizes, physical parameters and device pointers of its fields.  The same struct is the element of the
