@@ -412,7 +412,19 @@ int hf_obstacle_fields(const hf_plan* p, int all_scenes, void* stream) {
         hf::k_footprint<<<(sc.n_particles + hf::kThreads - 1) / hf::kThreads, hf::kThreads, 0, S(stream)>>>(scenes, s);
         hf::k_scatter<<<(sc.n_particles + hf::kThreads - 1) / hf::kThreads, hf::kThreads, 0, S(stream)>>>(scenes, s);
     }
-    if (p->num_chunks) {
+    if (!all_scenes) {
+        // the substep's rebuild: each coupled scene over its footprint boxes only
+        for (int s = 0; s < p->num_scenes; ++s) {
+            const hf_scene& sc = p->scenes_host[s];
+            if (!(sc.flags & HF_FLAG_ACTIVE) || !(sc.flags & HF_FLAG_PARTICLES) || sc.n_particles <= 0) continue;
+            hf::k_obstacle_box<<<296, hf::kThreads, 0, S(stream)>>>(scenes, s);
+        }
+        for (int s = 0; s < p->num_scenes; ++s) {
+            const hf_scene& sc = p->scenes_host[s];
+            if (!(sc.flags & HF_FLAG_ACTIVE) || !(sc.flags & HF_FLAG_PARTICLES) || sc.n_particles <= 0) continue;
+            hf::k_coeff_box<<<296, hf::kThreads, 0, S(stream)>>>(scenes, s);
+        }
+    } else if (p->num_chunks) {
         hf::k_obstacle<<<p->num_chunks, hf::kThreads, 0, S(stream)>>>(scenes, work, all_scenes);
         hf::k_coeff<<<p->num_chunks, hf::kThreads, 0, S(stream)>>>(scenes, work, all_scenes);
     }

@@ -43,6 +43,9 @@ __global__ void k_scatter(const hf_scene* __restrict__ scenes, int s);
 __global__ void k_footprint(const hf_scene* __restrict__ scenes, int s);
 __global__ void k_obstacle(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, int all_scenes);
 __global__ void k_coeff(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, int all_scenes);
+// the per-substep rebuild of one coupled scene, over its footprint boxes only
+__global__ void k_obstacle_box(const hf_scene* __restrict__ scenes, int s);
+__global__ void k_coeff_box(const hf_scene* __restrict__ scenes, int s);
 __global__ void k_prestage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt);
 __global__ void k_advect_T(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt);
 __global__ void k_particle_update(const hf_scene* __restrict__ scenes, int s);

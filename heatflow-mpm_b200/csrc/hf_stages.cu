@@ -121,6 +121,43 @@ __device__ __forceinline__ float plus_static(float a, const float* st, int idx) 
     return st ? __fadd_rn(a, __ldg(st + idx)) : a;
 }
 
+// One cell of the obstacle fields (grid.py:202-213 plus the particle sums; grid.py:62-67 wall fluxes).
+__device__ __forceinline__ void obstacle_cell(const hf_scene& S, bool particles, long long* acc, long long M, int t, int i,
+                                              int j, int k) {
+    const int n = S.n;
+    // cell lattices: alpha_s (+ static), alpha and tsum of the heat field
+    float a_s = particles ? take(acc, t) : 0.0f;
+    S.alpha_s[t] = plus_static(a_s, S.st_alpha, t);
+    S.alpha[t] = particles ? take(acc + 10 * M, t) : 0.0f;
+    S.tsum[t] = particles ? take(acc + 11 * M, t) : 0.0f;
+    // faces: low face of this cell, plus the high wall face on the last layer
+    const int fu[2] = {uidx(n, i, j, k), uidx(n, n, j, k)};
+    const int fv[2] = {vidx(n, i, j, k), vidx(n, i, n, k)};
+    const int fw[2] = {widx(n, i, j, k), widx(n, i, j, n)};
+    const bool hi[3] = {i == n - 1, j == n - 1, k == n - 1};
+    const bool lo_wall[3] = {i == 0, j == 0, k == 0};
+    float* q[3] = {S.qx, S.qy, S.qz};
+    float* kf[3] = {S.kx, S.ky, S.kz};
+    float* mf[3] = {S.mx, S.my, S.mz};
+    const float* stk[3] = {S.st_kx, S.st_ky, S.st_kz};
+    const float* stm[3] = {S.st_mx, S.st_my, S.st_mz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int* f = a == 0 ? fu : (a == 1 ? fv : fw);
+        for (int side = 0; side < 2; ++side) {
+            if (side == 1 && !hi[a]) break;
+            const int idx = f[side];
+            const bool wall = side == 1 || lo_wall[a];
+            float qv = particles ? take(acc + (1 + a) * M, idx) : 0.0f;
+            q[a][idx] = wall ? 0.0f : qv;
+            float kv = particles ? take(acc + (4 + a) * M, idx) : 0.0f;
+            kf[a][idx] = plus_static(kv, stk[a], idx);
+            float mv = particles ? take(acc + (7 + a) * M, idx) : 0.0f;
+            mf[a][idx] = plus_static(mv, stm[a], idx);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) k_obstacle(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
                                                       int all_scenes) {
     const WorkItem wi = work[blockIdx.x];
@@ -129,7 +166,6 @@ __global__ void __launch_bounds__(kThreads) k_obstacle(const hf_scene* __restric
     if (!particles && !all_scenes) return;
     const int n = S.n, N = n * n * n;
     const long long M = (long long)(n + 1) * (n + 1) * (n + 1);
-    long long* acc = S.acc;
     const int* bnow = S.state->box;
     const int* bprev = S.state->box_prev;
     for (int m = 0; m < kCellsPerThread; ++m) {
@@ -139,37 +175,37 @@ __global__ void __launch_bounds__(kThreads) k_obstacle(const hf_scene* __restric
         cell_ijk(t, n, i, j, k);
         // only the particles' footprint of this and the previous substep changes (the rest holds the static fields)
         if (!all_scenes && !in_box(bnow, i, j, k, 0) && !in_box(bprev, i, j, k, 0)) continue;
-        // cell lattices: alpha_s (+ static), alpha and tsum of the heat field
-        float a_s = particles ? take(acc, t) : 0.0f;
-        S.alpha_s[t] = plus_static(a_s, S.st_alpha, t);
-        S.alpha[t] = particles ? take(acc + 10 * M, t) : 0.0f;
-        S.tsum[t] = particles ? take(acc + 11 * M, t) : 0.0f;
-        // faces: low face of this cell, plus the high wall face on the last layer
-        const int fu[2] = {uidx(n, i, j, k), uidx(n, n, j, k)};
-        const int fv[2] = {vidx(n, i, j, k), vidx(n, i, n, k)};
-        const int fw[2] = {widx(n, i, j, k), widx(n, i, j, n)};
-        const bool hi[3] = {i == n - 1, j == n - 1, k == n - 1};
-        const bool lo_wall[3] = {i == 0, j == 0, k == 0};
-        float* q[3] = {S.qx, S.qy, S.qz};
-        float* kf[3] = {S.kx, S.ky, S.kz};
-        float* mf[3] = {S.mx, S.my, S.mz};
-        const float* stk[3] = {S.st_kx, S.st_ky, S.st_kz};
-        const float* stm[3] = {S.st_mx, S.st_my, S.st_mz};
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int* f = a == 0 ? fu : (a == 1 ? fv : fw);
-            for (int side = 0; side < 2; ++side) {
-                if (side == 1 && !hi[a]) break;
-                const int idx = f[side];
-                const bool wall = side == 1 || lo_wall[a];
-                float qv = particles ? take(acc + (1 + a) * M, idx) : 0.0f;
-                q[a][idx] = wall ? 0.0f : qv;
-                float kv = particles ? take(acc + (4 + a) * M, idx) : 0.0f;
-                kf[a][idx] = plus_static(kv, stk[a], idx);
-                float mv = particles ? take(acc + (7 + a) * M, idx) : 0.0f;
-                mf[a][idx] = plus_static(mv, stm[a], idx);
-            }
-        }
+        obstacle_cell(S, particles, S.acc, M, t, i, j, k);
+    }
+}
+
+// The bounding box of this and the previous substep's footprints grown by `grow` and clamped to the grid; false when
+// both are empty.  Every cell of it may be recomputed: outside the footprints the accumulators are zero and the
+// fields equal the statics, so a recomputation reproduces them.
+__device__ __forceinline__ bool footprint_union(const hf_scene& S, int grow, int (&lo)[3], int (&hi)[3]) {
+    const int* a = S.state->box;
+    const int* b = S.state->box_prev;
+    const bool ea = a[0] > a[3], eb = b[0] > b[3];
+    if (ea && eb) return false;
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = max(0, (ea ? b[d] : eb ? a[d] : min(a[d], b[d])) - grow);
+        hi[d] = min(S.n - 1, (ea ? b[3 + d] : eb ? a[3 + d] : max(a[3 + d], b[3 + d])) + grow);
+    }
+    return true;
+}
+
+// k_obstacle for one coupled scene over the footprint union only (the substep's rebuild)
+__global__ void __launch_bounds__(kThreads) k_obstacle_box(const hf_scene* __restrict__ scenes, int s) {
+    const hf_scene& S = scenes[s];
+    int lo[3], hi[3];
+    if (!footprint_union(S, 0, lo, hi)) return;
+    const int n = S.n;
+    const long long M = (long long)(n + 1) * (n + 1) * (n + 1);
+    const int ei = hi[0] - lo[0] + 1, ej = hi[1] - lo[1] + 1, ek = hi[2] - lo[2] + 1;
+    const int cells = ei * ej * ek;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cells; q += gridDim.x * blockDim.x) {
+        const int k = lo[2] + q % ek, j = lo[1] + (q / ek) % ej, i = lo[0] + q / (ek * ej);
+        obstacle_cell(S, true, S.acc, M, (i * n + j) * n + k, i, j, k);
     }
 }
 
@@ -181,6 +217,47 @@ __device__ __forceinline__ float conductivity(float a, float ka, float km) {
     return __fadd_rn(ka, __fmul_rn(__fsub_rn(km, ka), clampf_(__fdiv_rn(a, 0.6f), 0.0f, 1.0f)));
 }
 
+// One cell of the coefficient stage: conductivity (heat.py:44-47), face fractions (grid.py:46-59) and face
+// diffusivities (heat.py:50-53) of the cell's low faces (and the high wall faces on the last layer).
+__device__ __forceinline__ void coeff_cell(const hf_scene& S, float afmin, float ka, float km, const float* as, int t,
+                                           int i, int j, int k) {
+    const int n = S.n;
+    const float ac = as[t];
+    const float kc = conductivity(ac, ka, km);
+    S.kap[t] = kc;
+    const int fu = uidx(n, i, j, k), fv = vidx(n, i, j, k), fw = widx(n, i, j, k);
+    if (i == 0) {
+        S.ax[fu] = 0.0f;
+        S.hkx[fu] = 0.0f;
+    } else {
+        const float an = as[t - n * n];
+        S.ax[fu] = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
+        S.hkx[fu] = face_kappa(conductivity(an, ka, km), kc);
+    }
+    float ayv = 0.0f, azv = 0.0f;
+    if (j == 0) {
+        S.hky[fv] = 0.0f;
+    } else {
+        const float an = as[t - n];
+        ayv = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
+        S.hky[fv] = face_kappa(conductivity(an, ka, km), kc);
+    }
+    if (k == 0) {
+        S.hkz[fw] = 0.0f;
+    } else {
+        const float an = as[t - 1];
+        azv = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
+        S.hkz[fw] = face_kappa(conductivity(an, ka, km), kc);
+    }
+    S.ay[fv] = ayv;
+    S.az[fw] = azv;
+    S.ayc[t] = ayv;   // cell-layout copies for the tiled (TMA) pressure stencil
+    S.azc[t] = azv;
+    if (i == n - 1) S.ax[uidx(n, n, j, k)] = S.hkx[uidx(n, n, j, k)] = 0.0f;
+    if (j == n - 1) S.ay[vidx(n, i, n, k)] = S.hky[vidx(n, i, n, k)] = 0.0f;
+    if (k == n - 1) S.az[widx(n, i, j, n)] = S.hkz[widx(n, i, j, n)] = 0.0f;
+}
+
 __global__ void __launch_bounds__(kThreads) k_coeff(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
                                                    int all_scenes) {
     const WorkItem wi = work[blockIdx.x];
@@ -188,7 +265,6 @@ __global__ void __launch_bounds__(kThreads) k_coeff(const hf_scene* __restrict__
     if (!all_scenes && !(S.flags & HF_FLAG_PARTICLES)) return;
     const int n = S.n, N = n * n * n;
     const float afmin = (float)S.alpha_f_min, ka = (float)S.kappa_air, km = (float)S.kappa_mat;
-    const float* as = S.alpha_s;
     const int* bnow = S.state->box;
     const int* bprev = S.state->box_prev;
     for (int m = 0; m < kCellsPerThread; ++m) {
@@ -197,40 +273,22 @@ __global__ void __launch_bounds__(kThreads) k_coeff(const hf_scene* __restrict__
         int i, j, k;
         cell_ijk(t, n, i, j, k);
         if (!all_scenes && !in_box(bnow, i, j, k, 1) && !in_box(bprev, i, j, k, 1)) continue;
-        const float ac = as[t];
-        const float kc = conductivity(ac, ka, km);
-        S.kap[t] = kc;
-        const int fu = uidx(n, i, j, k), fv = vidx(n, i, j, k), fw = widx(n, i, j, k);
-        if (i == 0) {
-            S.ax[fu] = 0.0f;
-            S.hkx[fu] = 0.0f;
-        } else {
-            const float an = as[t - n * n];
-            S.ax[fu] = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
-            S.hkx[fu] = face_kappa(conductivity(an, ka, km), kc);
-        }
-        float ayv = 0.0f, azv = 0.0f;
-        if (j == 0) {
-            S.hky[fv] = 0.0f;
-        } else {
-            const float an = as[t - n];
-            ayv = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
-            S.hky[fv] = face_kappa(conductivity(an, ka, km), kc);
-        }
-        if (k == 0) {
-            S.hkz[fw] = 0.0f;
-        } else {
-            const float an = as[t - 1];
-            azv = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
-            S.hkz[fw] = face_kappa(conductivity(an, ka, km), kc);
-        }
-        S.ay[fv] = ayv;
-        S.az[fw] = azv;
-        S.ayc[t] = ayv;   // cell-layout copies for the tiled (TMA) pressure stencil
-        S.azc[t] = azv;
-        if (i == n - 1) S.ax[uidx(n, n, j, k)] = S.hkx[uidx(n, n, j, k)] = 0.0f;
-        if (j == n - 1) S.ay[vidx(n, i, n, k)] = S.hky[vidx(n, i, n, k)] = 0.0f;
-        if (k == n - 1) S.az[widx(n, i, j, n)] = S.hkz[widx(n, i, j, n)] = 0.0f;
+        coeff_cell(S, afmin, ka, km, S.alpha_s, t, i, j, k);
+    }
+}
+
+// k_coeff for one coupled scene over the footprint union grown by one cell (the substep's rebuild)
+__global__ void __launch_bounds__(kThreads) k_coeff_box(const hf_scene* __restrict__ scenes, int s) {
+    const hf_scene& S = scenes[s];
+    int lo[3], hi[3];
+    if (!footprint_union(S, 1, lo, hi)) return;
+    const int n = S.n;
+    const float afmin = (float)S.alpha_f_min, ka = (float)S.kappa_air, km = (float)S.kappa_mat;
+    const int ei = hi[0] - lo[0] + 1, ej = hi[1] - lo[1] + 1, ek = hi[2] - lo[2] + 1;
+    const int cells = ei * ej * ek;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < cells; q += gridDim.x * blockDim.x) {
+        const int k = lo[2] + q % ek, j = lo[1] + (q / ek) % ej, i = lo[0] + q / (ek * ej);
+        coeff_cell(S, afmin, ka, km, S.alpha_s, (i * n + j) * n + k, i, j, k);
     }
 }
 
