@@ -1,7 +1,8 @@
 // hf_api.cu -- host side of the C ABI declared in include/heatflow_b200.h.
 //
-// Stateless apart from a per-device cache of SM count and cooperative-launch occupancy.  No function allocates device
-// memory; the workspace layout below carves the caller's buffer.
+// Stateless apart from a per-device cache of SM count and cooperative-launch occupancies.  No function allocates device
+// memory; the workspace layout below carves the caller's buffer (barrier counters, offset tables, the scenes' TMA
+// descriptors, the CG partial sums).
 #include <algorithm>
 #include <cstdio>
 #include <cudaTypedefs.h>

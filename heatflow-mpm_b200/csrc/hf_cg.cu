@@ -20,11 +20,15 @@
 // recomputes it at the stencil points it reads from z and the previous p (double-buffered), so it costs no barrier.
 //
 // Variants:
-//   k_pcg       streaming: vectors in global memory, any number of scenes (batched and served plans).
+//   k_pcg       streaming: vectors in global memory, any number of scenes (batched and served plans).  The scenes come
+//               in L2-sized groups solved by the lanes of the grid; for the pressure system with every scene at
+//               n % 4 == 0 each tile's stencil boxes and CG vectors are staged by TMA from per-scene descriptors,
+//               double-buffered per block.  Optional outer defect correction (fp64 true residual, restart).
 //   k_pcg_res   register-resident, one scene: every thread keeps x, r, z, p, D and Ap of its cells in registers for
-//               the whole solve; only p and z are published (neighbouring blocks read them).  For the pressure system
-//               with n % 4 == 0 the stencil inputs of each tile -- z and the previous p with a one-cell halo, and the
-//               face fractions -- are staged into shared memory by TMA (cp.async.bulk.tensor) instead of gathered.
+//               the whole solve; only p and z are published (neighbouring blocks read them).
+//   k_pcg_tma   register-resident pressure solve of one scene with n % 4 == 0: the stencil inputs of each tile -- z
+//               and the previous p with a one-cell halo, and the face fractions -- are staged into shared memory by
+//               TMA (cp.async.bulk.tensor) instead of gathered; x, r and D stay in registers.
 #include <cuda.h>
 
 #include "hf_device.cuh"

@@ -139,7 +139,7 @@ typedef struct hf_plan {
     const hf_scene *scenes_host;   /* host copy, valid while the plan is used */
     void *scenes_dev;          /* device: hf_scene[num_scenes] */
     void *work_dev;            /* device: int32 pairs (scene, first cell) [num_chunks] */
-    void *workspace;           /* device: >= hf_workspace_bytes(num_scenes, num_chunks) bytes */
+    void *workspace;           /* device: >= hf_workspace_bytes(num_scenes, num_chunks, num_tiles) bytes */
     size_t workspace_bytes;
     int32_t persistent_blocks; /* grid of the persistent CG kernels (0 = choose: SMs x occupancy) */
     int32_t options;           /* HF_PLAN_* bits */
@@ -154,15 +154,17 @@ size_t hf_workspace_bytes(int num_scenes, int num_chunks, int num_tiles);
 /* number of 1024-cell chunks / 4x8x32 tiles of a scene of n cells per edge */
 int hf_chunks_for(int n);
 int hf_tiles_for(int n);
-/* Writes the scene table and the chunk and tile work tables to the device and fills plan.num_chunks/num_tiles.  Blocking: the stream is
- * synchronised before return (set-up call, not for the per-substep path). */
+/* Writes the scene table, the chunk and tile work tables and the scenes' TMA descriptors (into the workspace) to the
+ * device, fills plan.num_chunks/num_tiles and sets HF_PLAN_MAPS_READY.  Blocking: the stream is synchronised before
+ * return (set-up call, not for the per-substep path).  Call it again whenever a scene's buffers change. */
 int hf_plan_upload(hf_plan *plan, void *stream);
 
 /* --------------------------------------------------------------------------------- per-substep stages (batched) */
 /* solver.py:65-72 + grid.py:202-213 + grid.py:46-67 + heat.py:44-47: obstacle fields of every scene -- particle
  * scatter (k_scatter_particles solver.py:19-38, k_scatter_heat heat.py:12-18) into fixed-point accumulators, plus the
  * static heater fields, face fractions alpha_f with zeroed wall fluxes, and the conductivity kappa.  Scenes without
- * HF_FLAG_PARTICLES are skipped unless `all_scenes` is set (used once at set-up to fill their static fields). */
+ * HF_FLAG_PARTICLES are skipped unless `all_scenes` is set (used once at set-up to fill their static fields); per
+ * substep, a coupled scene is rebuilt only inside the footprint boxes of its particles (this and the previous substep). */
 int hf_obstacle_fields(const hf_plan *plan, int all_scenes, void *stream);
 /* solver.py:74-79 + heat.py:108-118: k_blend, k_apply_fixed, k_source (rate > 0), k_advect, k_heat_rhs */
 int hf_temperature_stage(const hf_plan *plan, double dt, void *stream);
