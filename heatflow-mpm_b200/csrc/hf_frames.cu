@@ -35,7 +35,28 @@ __global__ void __launch_bounds__(kThreads) k_pack_frame(const hf_scene* __restr
     }
 }
 
+// The current buffer (device-side parity) of T, u, v or w of scene s, copied into `out`.
+__global__ void __launch_bounds__(kThreads) k_current_field(const hf_scene* __restrict__ scenes, int s, int which,
+                                                            float* __restrict__ out) {
+    const hf_scene& S = scenes[s];
+    const int n = S.n, par = S.state->parity;
+    const long long N = (long long)n * n * n, F = (long long)(n + 1) * n * n;
+    const float* src = which == 0 ? S.T[par] : which == 1 ? S.u[par] : which == 2 ? S.v[par] : S.w[par];
+    const long long count = which == 0 ? N : F;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += (long long)gridDim.x * blockDim.x)
+        out[t] = src[t];
+}
+
 }  // namespace hf
+
+extern "C" int hf_current_field(const hf_plan* p, int s, int which, float* out, void* stream) {
+    if (!p || !p->scenes_dev || !p->scenes_host || s < 0 || s >= p->num_scenes || which < 0 || which > 3 || !out)
+        return hf::set_error(HF_ERR_ARG, "hf_current_field: bad plan, scene index, field or output");
+    hf::k_current_field<<<592, hf::kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const hf_scene*>(p->scenes_dev), s, which, out);
+    if (cudaGetLastError() != cudaSuccess) return hf::set_error(HF_ERR_CUDA, "hf_current_field: launch failed");
+    return HF_OK;
+}
 
 extern "C" int hf_pack_frame(const hf_plan* p, int s, void* grid_T, void* air_u, void* temp, void* melt, void* stream) {
     if (!p || !p->scenes_dev || !p->scenes_host || s < 0 || s >= p->num_scenes)

@@ -89,6 +89,7 @@ def load():
     for name in ("hf_cell_velocity", "hf_divergence_max", "hf_speed_max"):
         getattr(L, name).argtypes = [C.POINTER(Plan), C.c_int, _P, _P]
     L.hf_pack_frame.argtypes = [C.POINTER(Plan), C.c_int, _P, _P, _P, _P, _P]
+    L.hf_current_field.argtypes = [C.POINTER(Plan), C.c_int, C.c_int, _P, _P]
     L.hf_k_laplacian.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double] + [_P] * 6 + [_P]
     L.hf_k_heat_matvec.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double] + [_P] * 5 + [_P]
     if L.hf_abi_version() != 1:

@@ -11,6 +11,7 @@ from dataclasses import asdict
 import numpy as np
 import torch
 
+from . import _lib
 from .grid import AirGrid, GridConfig, grid_edge
 from .heat import HeatField
 from .heater import Heater
@@ -129,6 +130,34 @@ class HeatflowMPM:
             out.copy_(self.heat.T)
             return out
         return self.heat.T.cpu().numpy()
+
+    def grid_T_async(self, out):
+        """grid_T into `out` (a pinned host tensor of shape (n,n,n)) without waiting: the current temperature is copied
+        on the device into one of two staging buffers, then downloaded on a side stream while the next substeps run.
+        Returns a torch.cuda.Event that completes when `out` holds the data.  A staging buffer is refilled only after
+        its previous download finished, so at most two downloads are in flight."""
+        import ctypes as C
+        n = self.grid.n
+        if not hasattr(self, "_stage"):
+            self._stage = [torch.empty((n, n, n), dtype=torch.float32, device=self.dev) for _ in range(2)]
+            self._stage_done = [None, None]
+            self._stage_k = 0
+            self._copy_stream = torch.cuda.Stream(torch.device(self.dev))
+        k = self._stage_k % 2
+        self._stage_k += 1
+        compute = torch.cuda.current_stream(torch.device(self.dev))
+        if self._stage_done[k] is not None:
+            compute.wait_event(self._stage_done[k])
+        buf = self._stage[k]
+        _lib.check(self.plan.L.hf_current_field(C.byref(self.plan.plan), 0, 0, buf.data_ptr(),
+                                                C.c_void_p(compute.cuda_stream)), "hf_current_field")
+        self._copy_stream.wait_stream(compute)
+        with torch.cuda.stream(self._copy_stream):
+            out.copy_(buf, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(self._copy_stream)
+        self._stage_done[k] = done
+        return done
 
     def air_velocity(self):
         return self.grid.cell_velocity()

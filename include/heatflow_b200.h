@@ -196,6 +196,10 @@ int hf_speed_max(const hf_plan *plan, int s, float *out_dev, void *stream);
    (n^3 x 3, grid.py:156-162) and the particles' temperature and melt fraction (n_particles each) of scene `s`, converted
    to binary16 (round to nearest even, as numpy's astype(float16)) into device buffers; any output may be NULL */
 int hf_pack_frame(const hf_plan *plan, int s, void *grid_T, void *air_u, void *temp, void *melt, void *stream);
+/* solver.py:95-96 grid_T and the face velocities without a host read-back of the parity: the current buffer of
+   scene `s`'s T (which = 0: n^3 floats) or u, v, w (which = 1, 2, 3: (n+1) n^2 floats) copied into device memory `out`,
+   so that a caller can download it asynchronously while the next substeps run */
+int hf_current_field(const hf_plan *plan, int s, int which, float *out, void *stream);
 
 /* ------------------------------------------------------------- single-kernel entry points (parity, unit tests) */
 /* grid.py:94-115 k_laplacian: out = alpha * L(p) / h^2 + beta * y (n^3 arrays, one scene) */

@@ -69,3 +69,25 @@ def test_run_scene_cli(tmp_path):
     assert f["air_u"].shape == (n ** 3, 3) and f["temp"].dtype == np.float16 and f["pos"].dtype == np.float32
     assert float(f["t"]) == pytest.approx(0.06) and np.isfinite(f["grid_T"].astype(np.float32)).all()
     assert os.path.exists(os.path.join(out, "meta.json"))
+
+
+@pytest.mark.gpu
+def test_grid_T_async_matches_grid_T():
+    """grid_T_async (device-side copy of the current buffer, download on a side stream) delivers what grid_T reads,
+    through both staging buffers."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    from heatflow_mpm import GridConfig, Heater, HeatflowMPM, Material
+    from heatflow_mpm.synthetic import ellipsoid_particles
+    P = ellipsoid_particles(semi=(0.03, 0.02, 0.04), spacing=4e-3, L=0.24)
+    sim = HeatflowMPM(P, Material(), Heater(dist=0.1, z=0.06, radius=0.03, length=0.1, fan=2.0),
+                      GridConfig(L=0.24, h=0.01), 4e-3, 20.0, body="frozen")
+    n = sim.grid.n
+    bufs = [torch.empty((n, n, n), dtype=torch.float32).pin_memory() for _ in range(2)]
+    for k in range(5):
+        sim.substep(2e-3)
+        ev = sim.grid_T_async(bufs[k % 2])
+        ref = sim.grid_T()
+        ev.synchronize()
+        assert np.array_equal(bufs[k % 2].numpy(), ref), k
