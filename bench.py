@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--streaming", default="none", choices=["none", "heat", "both"],
                     help="plain: CG solves in the streaming kernel instead of the resident one")
     ap.add_argument("--persistent-blocks", type=int, default=0, help="plain: grid of the streaming CG kernel")
+    ap.add_argument("--no-tma", action="store_true", help="plain: resident pressure CG without the TMA-staged stencil")
     ap.add_argument("--scenes", type=int, default=64, help="batched: scenes in the ensemble")
     ap.add_argument("--graph-steps", type=int, default=10, help="batched: substeps per captured CUDA graph")
     ap.add_argument("--edges", default="32,48,64,96,128", help="batched: grid edges the ensemble draws from")
@@ -299,6 +300,8 @@ def bench_plain(args, dev, rank, world, local):
     plan.plan.persistent_blocks = args.persistent_blocks
     from heatflow_mpm import _lib as L_
     plan.plan.options |= {"none": 0, "heat": L_.HF_PLAN_STREAMING_HEAT, "both": L_.HF_PLAN_STREAMING_CG}[args.streaming]
+    if args.no_tma:
+        plan.plan.options |= L_.HF_PLAN_NO_TMA
     n = sim.grid.n
     N = n ** 3
     stream = torch.cuda.current_stream()

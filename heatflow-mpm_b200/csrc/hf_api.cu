@@ -155,7 +155,40 @@ int encode_map(CUtensorMap* m, const float* base, int nk, int nj, int ni, int bk
 
 // The six TMA descriptors of a scene's tiled pressure stencil (order of hf::TileMaps): z and both search-direction
 // buffers with a one-cell halo, alpha_f x on its face lattice, alpha_f y and z in cell layout.
-static_assert(sizeof(hf::TileMaps) == 6 * sizeof(CUtensorMap), "TileMaps is six consecutive descriptors");
+static_assert(sizeof(hf::TileMaps) == 10 * sizeof(CUtensorMap), "TileMaps is ten consecutive descriptors");
+
+// a 3-D byte array (k fastest) of dims (nk, nj, ni) with a box (bk, bj, bi): nk and bk multiples of 16
+int encode_map_u8(CUtensorMap* m, const uint8_t* base, int nk, int nj, int ni, int bk, int bj, int bi) {
+    if (!g_encode) {
+        CUtensorMap probe;
+        int rc = encode_map(&probe, reinterpret_cast<const float*>(base), 4, 1, 1, 4, 1, 1);   // loads the entry point
+        if (rc) return rc;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)nk, (cuuint64_t)nj, (cuuint64_t)ni};
+    const cuuint64_t strides[2] = {(cuuint64_t)nk, (cuuint64_t)nk * nj};
+    const cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)bj, (cuuint32_t)bi};
+    const cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(base), dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(HF_ERR_DEVICE, "cuTensorMapEncodeTiled (bytes) failed");
+    return HF_OK;
+}
+
+// The TMA descriptors of a scene's tiled heat stencil: the z / p boxes of the pressure geometry, the face
+// diffusivities x (face lattice, like alpha_f x), y (rows j0..j0+8 of the (n, n+1, n) face lattice) and z (cell-layout
+// copy), and the cell flags with a one-cell halo (k origin 16-byte aligned).  Needs n % 16 == 0 (byte rows).
+int encode_heat_maps(const hf_scene& sc, hf::TileMaps& m) {
+    const int n = sc.n;
+    int rc;
+    if ((rc = encode_map(&m.z, sc.cg_z, n, n, n, 40, 10, 6))) return rc;
+    if ((rc = encode_map(&m.p0, sc.cg_p[0], n, n, n, 40, 10, 6))) return rc;
+    if ((rc = encode_map(&m.p1, sc.cg_p[1], n, n, n, 40, 10, 6))) return rc;
+    if ((rc = encode_map(&m.hkx, sc.hkx, n, n, n + 1, 32, 8, 5))) return rc;
+    if ((rc = encode_map(&m.hky, sc.hky, n, n + 1, n, 32, 9, 4))) return rc;
+    if ((rc = encode_map(&m.hkzc, sc.hkzc, n, n, n, 36, 8, 4))) return rc;
+    return encode_map_u8(&m.flags, sc.cell_flags, n, n, n, 64, 10, 6);
+}
 
 int encode_scene_maps(const hf_scene& sc, CUtensorMap* m) {
     const int n = sc.n;
@@ -196,13 +229,15 @@ int launch_resident(const hf_plan* p, DeviceInfo* d, bool heat, double dt, int s
     const int nt = t_hi - t_lo;
     const int G = nt < d->sms ? nt : d->sms;
     const int tpb = (nt + G - 1) / G;
-    const bool tma = !heat && (sc.n % 4 == 0) && !(p->options & HF_PLAN_NO_TMA);
+    // TMA-staged stencils: pressure with n % 4 == 0 (16-byte float rows), heat with n % 16 == 0 (16-byte flag rows)
+    const bool tma = !(p->options & HF_PLAN_NO_TMA) &&
+                     (heat ? (sc.n % 16 == 0 && sc.hkzc && sc.hkx && sc.hky && sc.cell_flags) : (sc.n % 4 == 0));
     const int want = (int)((p->options >> HF_PLAN_RES_TILES_SHIFT) & 3u);   // 0: the first that fits
     for (int m = want ? want : 1; m <= 3; ++m) {
         const int groups = (tpb + m - 1) / m;
         if (groups > kResGroupsMax[m]) continue;
         const void* fn = hf::pcg_resident_kernel(heat, m, tma);
-        const size_t smem = hf::pcg_resident_smem(groups, m, tma);
+        const size_t smem = hf::pcg_resident_smem(groups, m, tma, heat);
         if (smem > d->smem_optin) continue;
         int& occ = d->res_occ[heat][m][tma][groups];
         if (occ < 0) {
@@ -215,7 +250,7 @@ int launch_resident(const hf_plan* p, DeviceInfo* d, bool heat, double dt, int s
         if (occ < 1) continue;
         hf::TileMaps maps;
         std::memset(&maps, 0, sizeof maps);
-        if (tma && (rc = encode_scene_maps(sc, &maps.z))) return rc;
+        if (tma && (rc = heat ? encode_heat_maps(sc, maps) : encode_scene_maps(sc, &maps.z))) return rc;
         HF_CUDA(cudaMemsetAsync(ws.bar, 0, kHeadBytes, S(stream)), "cudaMemsetAsync(barrier)");
         void* args[] = {(void*)&scenes, (void*)&tiles, (void*)&t_lo, (void*)&t_hi, (void*)&dt, (void*)&ws, (void*)&maps};
         HF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(256 * groups), args, smem, S(stream)),

@@ -432,6 +432,11 @@ __device__ __forceinline__ void write_stats(const hf_scene& S, const LocalScene&
 // Out-of-range elements are zero-filled by the copy engine and never used (domain faces are skipped).
 constexpr int kBZ = 40 * 10 * 6, kBX = 32 * 8 * 5, kBY = 32 * 9 * 4, kBW = 36 * 8 * 4;
 constexpr int kSlotFloats = 2 * kBZ + kBX + kBY + kBW;   // 8384 floats = 33,536 bytes (a multiple of 128)
+// Heat system: the same z / p boxes; face diffusivities x (face lattice), y (face lattice: rows j0..j0+8 of (n, n+1, n))
+// and z (cell-layout copy) in the face-fraction places; the cell flags (bytes) k in [k0-16, k0+48), j in [j0-1, j0+9),
+// i in [i0-1, i0+5) -- 16-byte aligned k origin; the owner's and the neighbours' fixed bits.
+constexpr int kBF = 64 * 10 * 6;                                   // bytes
+constexpr int kHeatSlotFloats = kSlotFloats + kBF / 4;             // 9344 floats = 37,376 bytes (a multiple of 128)
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -1273,11 +1278,12 @@ finish:
 // of the own cells is read from the staged box (its centre), A p is parked in the p_{k-1} box (dead once p_k is
 // formed), so a thread keeps only x, r and D of its cells in registers.  One group reduction per phase covers all the
 // thread's tiles.
-template <int MAXC>
+template <bool HEAT, int MAXC>
 __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     k_pcg_tma(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int tile_lo, int tile_hi,
               double dt_d, Workspace ws, const __grid_constant__ TileMaps maps) {
     constexpr int CPT = 4 * MAXC;
+    constexpr int SLOT = HEAT ? kHeatSlotFloats : kSlotFloats;
     extern __shared__ __align__(128) float sm_raw[];
     float* sm_boxes = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
     __shared__ double red[kRedComps * 32];
@@ -1290,13 +1296,13 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     const hf_scene& S = scenes[sidx];
     const int n = S.n, N = n * n * n;
     const int par = S.state->parity;
-    unsigned* bar = ws.bar + kMaxLanes;
+    unsigned* bar = ws.bar + (HEAT ? 0 : kMaxLanes);
     unsigned epoch = 0;
-    const float h = (float)S.h, hh = __fmul_rn(h, h);
+    const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn((float)dt_d, hh);
     double* bufA = ws.partA;
     double* bufB = ws.partB;
     const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
-    float* xg = S.p;
+    float* xg = HEAT ? S.T[par ^ 1] : S.p;
     float* zg = S.cg_z;
     TileItem my[MAXC];
     bool have[MAXC];
@@ -1315,8 +1321,8 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     __syncthreads();
     float x[CPT], r[CPT], D[CPT];
     // ------------------------------------------------------------------------------------------ prologue
-    float mean;
-    {
+    float mean = 0.0f;
+    if (!HEAT) {
         double mm[1];
         const int comp[1] = {0};
         scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red);
@@ -1334,7 +1340,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 const Cell cl = tile_cell(my[q], n, lt, m);
                 if (!have[q] || !cl.ok) continue;
                 float b, d, rr;
-                setup_cell<false>(S, xg, mean, hh, 0.0f, cl, b, d, rr);
+                setup_cell<HEAT>(S, xg, mean, hh, c_dt, cl, b, d, rr);
                 const float z = __fmul_rn(d, rr);
                 x[s] = xg[cl.t];
                 D[s] = d;
@@ -1356,17 +1362,20 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             }
         }
     }
-    // the face fractions of the tiles stay in shared memory for the whole solve
+    // the tiles' face coefficients stay in shared memory for the whole solve: face fractions (pressure), or the face
+    // diffusivities and the fixed-cell flags with a one-cell halo (heat)
     if (lt == 0) {
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) {
             if (!have[q]) continue;
-            float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+            float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
             unsigned long long* mb = &mbar[g * MAXC + q];
-            mbar_expect_tx(mb, (unsigned)((kBX + kBY + kBW) * sizeof(float)));
-            tma_load_3d(slot + 2 * kBZ, &maps.ax, my[q].k0, my[q].j0, my[q].i0, mb);
-            tma_load_3d(slot + 2 * kBZ + kBX, &maps.ayc, my[q].k0, my[q].j0, my[q].i0, mb);
-            tma_load_3d(slot + 2 * kBZ + kBX + kBY, &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
+            mbar_expect_tx(mb, (unsigned)((kBX + kBY + kBW) * sizeof(float) + (HEAT ? kBF : 0)));
+            tma_load_3d(slot + 2 * kBZ, HEAT ? &maps.hkx : &maps.ax, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + 2 * kBZ + kBX, HEAT ? &maps.hky : &maps.ayc, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + 2 * kBZ + kBX + kBY, HEAT ? &maps.hkzc : &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
+            if (HEAT)
+                tma_load_3d(slot + 2 * kBZ + kBX + kBY + kBW, &maps.flags, my[q].k0 - 16, my[q].j0 - 1, my[q].i0 - 1, mb);
         }
     }
     {
@@ -1383,7 +1392,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         const int comp[3] = {0, 1, 2};
         scene_sums<3>(bufB, cb, ce, comp, tot, red);
         if (threadIdx.x == 0) {
-            init_scalars(Ls, S, false, tot, N);
+            init_scalars(Ls, S, HEAT, tot, N);
             Ls.mean = (double)mean;
         }
         __syncthreads();
@@ -1400,7 +1409,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
                 if (!have[q]) continue;
-                float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
                 unsigned long long* mb = &mbar[g * MAXC + q];
                 mbar_expect_tx(mb, (unsigned)((first ? 1 : 2) * kBZ * sizeof(float)));
                 tma_load_3d(slot, &maps.z, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
@@ -1421,7 +1430,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
                 if (!have[q]) continue;
-                float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
                 for (int e = lt; e < kBZ; e += 256) slot[e] = __fadd_rn(slot[e], __fmul_rn(beta, slot[kBZ + e]));
             }
         }
@@ -1431,7 +1440,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
                 part[q] = 0.0;
-                float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
                 const float* Pb = slot;
                 float* Apb = slot + kBZ;   // the p_{k-1} box is dead now: A p goes to its centre
                 const float* axb = slot + 2 * kBZ;
@@ -1444,17 +1453,56 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                     const int bi = m, bj = lt >> 5, bk = lt & 31;
                     const int o = (bi + 1) * 400 + (bj + 1) * 40 + (bk + 4);
                     const float pc = Pb[o];
-                    float acc = 0.0f;
-                    if (cl.i > 0) acc = __fadd_rn(acc, __fmul_rn(axb[bi * 256 + bj * 32 + bk], __fsub_rn(pc, Pb[o - 400])));
-                    if (cl.i < n - 1)
-                        acc = __fadd_rn(acc, __fmul_rn(axb[(bi + 1) * 256 + bj * 32 + bk], __fsub_rn(pc, Pb[o + 400])));
-                    if (cl.j > 0) acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + bj * 32 + bk], __fsub_rn(pc, Pb[o - 40])));
-                    if (cl.j < n - 1)
-                        acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + (bj + 1) * 32 + bk], __fsub_rn(pc, Pb[o + 40])));
-                    if (cl.k > 0) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk], __fsub_rn(pc, Pb[o - 1])));
-                    if (cl.k < n - 1)
-                        acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk + 1], __fsub_rn(pc, Pb[o + 1])));
-                    const float ap = __fdiv_rn(acc, hh);
+                    float ap;
+                    if (HEAT) {
+                        // heat.py:94-105 with heat.py:55-91 neighbour_terms (use_fixed = 0): identity rows on fixed
+                        // cells, fixed neighbours enter as kappa_f x_c
+                        const unsigned char* flb = reinterpret_cast<const unsigned char*>(azb + kBW);
+                        const int of = (bi + 1) * 640 + (bj + 1) * 64 + (bk + 16);
+                        if (flb[of] & 1) {
+                            ap = pc;
+                        } else {
+                            float acc = 0.0f;
+                            float kf;
+                            if (cl.i > 0) {
+                                kf = axb[bi * 256 + bj * 32 + bk];
+                                acc = __fadd_rn(acc, (flb[of - 640] & 1) ? __fmul_rn(kf, pc) : __fmul_rn(kf, __fsub_rn(pc, Pb[o - 400])));
+                            }
+                            if (cl.i < n - 1) {
+                                kf = axb[(bi + 1) * 256 + bj * 32 + bk];
+                                acc = __fadd_rn(acc, (flb[of + 640] & 1) ? __fmul_rn(kf, pc) : __fmul_rn(kf, __fsub_rn(pc, Pb[o + 400])));
+                            }
+                            if (cl.j > 0) {
+                                kf = ayb[bi * 288 + bj * 32 + bk];
+                                acc = __fadd_rn(acc, (flb[of - 64] & 1) ? __fmul_rn(kf, pc) : __fmul_rn(kf, __fsub_rn(pc, Pb[o - 40])));
+                            }
+                            if (cl.j < n - 1) {
+                                kf = ayb[bi * 288 + (bj + 1) * 32 + bk];
+                                acc = __fadd_rn(acc, (flb[of + 64] & 1) ? __fmul_rn(kf, pc) : __fmul_rn(kf, __fsub_rn(pc, Pb[o + 40])));
+                            }
+                            if (cl.k > 0) {
+                                kf = azb[bi * 288 + bj * 36 + bk];
+                                acc = __fadd_rn(acc, (flb[of - 1] & 1) ? __fmul_rn(kf, pc) : __fmul_rn(kf, __fsub_rn(pc, Pb[o - 1])));
+                            }
+                            if (cl.k < n - 1) {
+                                kf = azb[bi * 288 + bj * 36 + bk + 1];
+                                acc = __fadd_rn(acc, (flb[of + 1] & 1) ? __fmul_rn(kf, pc) : __fmul_rn(kf, __fsub_rn(pc, Pb[o + 1])));
+                            }
+                            ap = __fadd_rn(pc, __fmul_rn(c_dt, acc));
+                        }
+                    } else {
+                        float acc = 0.0f;
+                        if (cl.i > 0) acc = __fadd_rn(acc, __fmul_rn(axb[bi * 256 + bj * 32 + bk], __fsub_rn(pc, Pb[o - 400])));
+                        if (cl.i < n - 1)
+                            acc = __fadd_rn(acc, __fmul_rn(axb[(bi + 1) * 256 + bj * 32 + bk], __fsub_rn(pc, Pb[o + 400])));
+                        if (cl.j > 0) acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + bj * 32 + bk], __fsub_rn(pc, Pb[o - 40])));
+                        if (cl.j < n - 1)
+                            acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + (bj + 1) * 32 + bk], __fsub_rn(pc, Pb[o + 40])));
+                        if (cl.k > 0) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk], __fsub_rn(pc, Pb[o - 1])));
+                        if (cl.k < n - 1)
+                            acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk + 1], __fsub_rn(pc, Pb[o + 1])));
+                        ap = __fdiv_rn(acc, hh);
+                    }
                     Apb[o] = ap;
                     pnew[cl.t] = pc;
                     part[q] += (double)pc * (double)ap;
@@ -1485,7 +1533,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
                 part[2 * q] = part[2 * q + 1] = 0.0;
-                const float* slot = sm_boxes + (size_t)(g * MAXC + q) * kSlotFloats;
+                const float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
                     const int s = q * 4 + m;
@@ -1515,11 +1563,11 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             double tot[2];
             const int comp[2] = {1, 2};
             scene_sums<2>(bufB, cb, ce, comp, tot, red);
-            if (threadIdx.x == 0) update_scalars(Ls, false, tot[0], tot[1], kit);
+            if (threadIdx.x == 0) update_scalars(Ls, HEAT, tot[0], tot[1], kit);
             __syncthreads();
         }
     }
-    // ------------------------------------------------------------------ write p back, then project the faces
+    // -------------------------------------------------- write x back, then (pressure) project the faces
 #pragma unroll
     for (int q = 0; q < MAXC; ++q) {
 #pragma unroll
@@ -1528,8 +1576,8 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             if (have[q] && cl.ok) xg[cl.t] = x[q * 4 + m];
         }
     }
-    if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
-    {
+    if (!HEAT) {
+        if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
         const float dtr = (float)(dt_d / S.rho);
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) {
@@ -1548,7 +1596,7 @@ finish:
         for (int q = 0; q < MAXC; ++q)
             if (have[q]) mbar_wait(&mbar[g * MAXC + q], phase_bit ^ 1u);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, false, *(volatile int*)ws.err != 0, par);
+    if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, HEAT, *(volatile int*)ws.err != 0, par);
 }
 
 const void* pcg_kernel(bool heat, bool tma) {
@@ -1558,23 +1606,28 @@ const void* pcg_kernel(bool heat, bool tma) {
 size_t pcg_stream_smem(bool tma) { return tma ? 2 * (size_t)kSlotFloats * sizeof(float) + 128 : 0; }
 
 const void* pcg_resident_kernel(bool heat, int maxc, bool tma) {
+    if (heat && tma) {
+        if (maxc == 1) return (const void*)k_pcg_tma<true, 1>;
+        if (maxc == 2) return (const void*)k_pcg_tma<true, 2>;
+        return (const void*)k_pcg_tma<true, 3>;
+    }
     if (heat) {
         if (maxc == 1) return (const void*)k_pcg_res<true, 1, false>;
         if (maxc == 2) return (const void*)k_pcg_res<true, 2, false>;
         return (const void*)k_pcg_res<true, 3, false>;
     }
     if (tma) {
-        if (maxc == 1) return (const void*)k_pcg_tma<1>;
-        if (maxc == 2) return (const void*)k_pcg_tma<2>;
-        return (const void*)k_pcg_tma<3>;
+        if (maxc == 1) return (const void*)k_pcg_tma<false, 1>;
+        if (maxc == 2) return (const void*)k_pcg_tma<false, 2>;
+        return (const void*)k_pcg_tma<false, 3>;
     }
     if (maxc == 1) return (const void*)k_pcg_res<false, 1, false>;
     if (maxc == 2) return (const void*)k_pcg_res<false, 2, false>;
     return (const void*)k_pcg_res<false, 3, false>;
 }
 
-size_t pcg_resident_smem(int groups, int maxc, bool tma) {
-    return tma ? (size_t)groups * maxc * kSlotFloats * sizeof(float) + 128 : 0;
+size_t pcg_resident_smem(int groups, int maxc, bool tma, bool heat) {
+    return tma ? (size_t)groups * maxc * (heat ? kHeatSlotFloats : kSlotFloats) * sizeof(float) + 128 : 0;
 }
 
 }  // namespace hf

@@ -36,7 +36,8 @@ struct Workspace {
 // TMA descriptors of the tiled pressure stencil (resident CG): z, both search-direction buffers, alpha_f x (the u
 // lattice), and the cell-layout copies of alpha_f y and z.
 struct TileMaps {
-    CUtensorMap z, p0, p1, ax, ayc, azc;
+    CUtensorMap z, p0, p1, ax, ayc, azc;      // pressure (and the z / p boxes of the heat system)
+    CUtensorMap hkx, hky, hkzc, flags;        // heat: face diffusivities and the cell flags (bytes)
 };
 
 __global__ void k_scatter(const hf_scene* __restrict__ scenes, int s);
@@ -71,7 +72,7 @@ size_t pcg_stream_smem(bool tma);
 // arguments: (const hf_scene*, const TileItem*, int tile_lo, int tile_hi, double dt, Workspace, TileMaps) -- the
 // scene's tiles; the TileMaps is used when tma; dynamic shared memory pcg_resident_smem(...)
 const void* pcg_resident_kernel(bool heat, int maxc, bool tma);
-size_t pcg_resident_smem(int groups, int maxc, bool tma);
+size_t pcg_resident_smem(int groups, int maxc, bool tma, bool heat);
 // device addresses of the per-scene chunk and tile offset tables inside a plan's workspace
 void plan_offset_tables(const hf_plan* p, int** chunk_begin, int** tile_begin);
 // record `msg` as the text of hf_last_error() and return `code`

@@ -242,13 +242,14 @@ __device__ __forceinline__ void coeff_cell(const hf_scene& S, float afmin, float
         ayv = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
         S.hky[fv] = face_kappa(conductivity(an, ka, km), kc);
     }
-    if (k == 0) {
-        S.hkz[fw] = 0.0f;
-    } else {
+    float hkzv = 0.0f;
+    if (k != 0) {
         const float an = as[t - 1];
         azv = clampf_(__fsub_rn(1.0f, __fmul_rn(0.5f, __fadd_rn(an, ac))), afmin, 1.0f);
-        S.hkz[fw] = face_kappa(conductivity(an, ka, km), kc);
+        hkzv = face_kappa(conductivity(an, ka, km), kc);
     }
+    S.hkz[fw] = hkzv;
+    if (S.hkzc) S.hkzc[t] = hkzv;   // cell-layout copy for the tiled (TMA) heat stencil
     S.ay[fv] = ayv;
     S.az[fw] = azv;
     S.ayc[t] = ayv;   // cell-layout copies for the tiled (TMA) pressure stencil

@@ -50,7 +50,7 @@ class Scene(C.Structure):
                [(f, _P) for f in SCENE_PTRS[:31]] + \
                [("cg_r", _P), ("cg_z", _P), ("cg_p", _P * 2), ("cg_Ap", _P),
                 ("pos", _P), ("pvel", _P), ("ptemp", _P), ("pmelt", _P), ("pyield", _P), ("pvisc", _P),
-                ("hkx", _P), ("hky", _P), ("hkz", _P), ("ayc", _P), ("azc", _P), ("acc", _P), ("state", _P)]
+                ("hkx", _P), ("hky", _P), ("hkz", _P), ("ayc", _P), ("azc", _P), ("hkzc", _P), ("acc", _P), ("state", _P)]
 
 
 class Plan(C.Structure):

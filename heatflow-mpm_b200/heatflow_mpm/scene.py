@@ -83,7 +83,7 @@ class DeviceScene:
         self.cg_p = [z(n, n, n), z(n, n, n)]
         self.ax, self.ay, self.az = (z(*s) for s in fs)
         self.hk = [z(*s) for s in fs]
-        self.ayc, self.azc = z(n, n, n), z(n, n, n)
+        self.ayc, self.azc, self.hkzc = z(n, n, n), z(n, n, n), z(n, n, n)
         self.cell_flags = z(n, n, n, dtype=torch.uint8)
         coupled = spec.n_particles > 0
         has_static = spec.static_alpha is not None
@@ -193,7 +193,7 @@ class DeviceScene:
         r.cg_p[0], r.cg_p[1] = P(s.cg_p[0]), P(s.cg_p[1])
         r.pos, r.pvel, r.ptemp, r.pmelt, r.pyield, r.pvisc = (P(a) for a in (s.pos, s.pvel, s.ptemp, s.pmelt, s.pyield, s.pvisc))
         r.hkx, r.hky, r.hkz = (P(a) for a in s.hk)
-        r.ayc, r.azc = P(s.ayc), P(s.azc)
+        r.ayc, r.azc, r.hkzc = P(s.ayc), P(s.azc), P(s.hkzc)
         r.acc = P(s.acc)
         r.state = P(s.state)
 

@@ -110,6 +110,8 @@ typedef struct hf_scene {
     float *hkx, *hky, *hkz;
     /* alpha_f of the low y and z face of every cell in cell layout (n,n,n) (copies of ay, az for tiled loads) */
     float *ayc, *azc;
+    /* the heat diffusivity of the low z face of every cell in cell layout (n,n,n) (a copy of hkz for tiled loads) */
+    float *hkzc;
     /* 12 fixed-point accumulators of (n+1)^3 int64 each (coupled scenes only), zero on entry, left zero */
     long long *acc;
     hf_scene_state *state;
