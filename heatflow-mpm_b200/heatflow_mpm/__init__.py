@@ -4,5 +4,8 @@ from .heat import HeatField  # noqa: F401
 from .heater import Heater, BoxHeater  # noqa: F401
 from .mpm import Material, ThermalMPM, FrozenBody  # noqa: F401
 from .solver import HeatflowMPM, KAPPA_AIR  # noqa: F401
+from .batch import AirScenario, AirBatch, autotune, ensemble, shard_scenarios  # noqa: F401
+from .serve import AirServer, Request, poisson_trace  # noqa: F401
+from .frames import FrameWriter  # noqa: F401
 
-__version__ = "0.2.0"
+__version__ = "0.3.0"
