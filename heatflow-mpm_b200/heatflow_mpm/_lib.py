@@ -60,6 +60,19 @@ class Plan(C.Structure):
                 ("options", C.c_int32)]
 
 
+class HeaterGeometry(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("fan", C.c_int32), ("centre", C.c_double * 3), ("facing", C.c_double * 3),
+                ("axis", C.c_double * 3), ("up", C.c_double * 3)] + \
+               [(f, C.c_double) for f in ("half_length", "shell_in", "shell_out", "cap_half", "cap_radius", "rod_half",
+                                          "rod_radius", "rod_front", "rod_dz", "fan_half", "fan_high", "fan_depth",
+                                          "trough_half", "trough_radius")] + \
+               [("box_lo", C.c_int32 * 3), ("box_hi", C.c_int32 * 3), ("box_trough", C.c_int32), ("sphere", C.c_int32),
+                ("t_rod", C.c_double), ("t_amb", C.c_double), ("m_face", C.c_float * 3), ("k_solid", C.c_float),
+                ("k_fan", C.c_float), ("sphere_t", C.c_float), ("sphere_lo", C.c_int32), ("sphere_hi", C.c_int32),
+                ("sphere_top", C.c_int32), ("pad_", C.c_int32), ("sphere_c", C.c_double), ("sphere_zc", C.c_double),
+                ("sphere_rr", C.c_double)]
+
+
 _lib = None
 
 
@@ -90,6 +103,8 @@ def load():
         getattr(L, name).argtypes = [C.POINTER(Plan), C.c_int, _P, _P]
     L.hf_pack_frame.argtypes = [C.POINTER(Plan), C.c_int, _P, _P, _P, _P, _P]
     L.hf_current_field.argtypes = [C.POINTER(Plan), C.c_int, C.c_int, _P, _P]
+    L.hf_scene_statics.argtypes = [C.POINTER(HeaterGeometry), C.c_int, C.c_double] + [_P] * 11 + [_P]
+    L.hf_winding_inside.argtypes = [_P, C.c_int, _P, C.c_int, C.c_float, _P, _P, _P]
     L.hf_k_laplacian.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double] + [_P] * 6 + [_P]
     L.hf_k_heat_matvec.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double] + [_P] * 5 + [_P]
     if L.hf_abi_version() != 1:

@@ -25,6 +25,7 @@ from . import _lib
 from .heater import FAN, K_SOLID, BoxHeater, Heater, face_masks, fan_momentum, source_rate
 from .scene import DeviceScene, SceneSpec, ScenePlan
 from .solver import wall_fixed
+from .voxelize import device_statics, sphere_bounds
 
 
 @dataclass
@@ -69,8 +70,7 @@ class AirScenario:
             # faces, cells held at sphere_t
             R, c = self.sphere_radius, self.L / 2
             x = (np.arange(n) + 0.5) * h
-            lo, hi = max(0, int((c - R) / h) - 1), min(n, int((c + R) / h) + 2)
-            top = min(n, int(2 * R / h) + 2)
+            lo, hi, top = sphere_bounds(n, h, self.L, R)
             ball = np.zeros((n, n, n), bool)
             ball[lo:hi, lo:hi, :top] = ((x[lo:hi, None, None] - c) ** 2 + (x[None, lo:hi, None] - c) ** 2
                                         + (x[None, None, :top] - R) ** 2 <= R * R)
@@ -83,6 +83,15 @@ class AirScenario:
                 mf[axis] = np.where(on_ball[axis], np.float32(0.0), mf[axis]).astype(np.float32)
         return SceneSpec(n=n, h=h, t_amb=self.t_amb, cg_tol=self.cg_tol, heat_tol=self.heat_tol, fixed=fixed, tfix=tfix,
                          source=g["source"], rate=rate, t_cap=self.t_cap, static_alpha=solid, static_k=kf, static_m=mf)
+
+    def device_spec(self, device="cuda:0") -> SceneSpec:
+        """spec() with the heater, walls and sphere voxelised on the device (voxelize.device_statics): the same
+        arrays bit for bit, without building or uploading them on the host."""
+        sphere = (self.sphere_radius, self.sphere_t, self.L) if self.sphere_radius > 0 else None
+        st = device_statics(self.heater(), self.n, self.h, (self.L / 2, self.L / 2), 1.2, self.t_amb, sphere=sphere,
+                            device=device)
+        return SceneSpec(n=self.n, h=self.h, t_amb=self.t_amb, cg_tol=self.cg_tol, heat_tol=self.heat_tol, rate=st.rate,
+                         t_cap=self.t_cap, statics=st)
 
     def initial_T(self):
         rng = np.random.default_rng(self.seed)
@@ -114,8 +123,11 @@ def _geometry(n, L, heater_x, fan_on, t_amb):
     return g
 
 
-def make_scene(sc: AirScenario, device="cuda:0") -> DeviceScene:
-    ds = DeviceScene(sc.spec(), device)
+def make_scene(sc: AirScenario, device="cuda:0", setup="device") -> DeviceScene:
+    """A resident scene of the scenario, its statics built on the device (setup="device") or on the host ("host")."""
+    if setup not in ("device", "host"):
+        raise ValueError("setup must be 'device' or 'host'")
+    ds = DeviceScene(sc.device_spec(device) if setup == "device" else sc.spec(), device)
     ds.set_current("T", sc.initial_T())
     ds.apply_fixed_to_T()
     return ds
@@ -241,10 +253,13 @@ def shard_scenarios(scenarios, rank, world):
     return [scenarios[i] for i in sorted(mine)]
 
 
-def upload_bytes(sc: AirScenario) -> int:
-    """Host-to-device bytes of creating the scene: initial T, fixed values, cell flags, static alpha and face weights."""
+def upload_bytes(sc: AirScenario, setup="device") -> int:
+    """Host-to-device bytes of creating the scene: the initial T, plus (statics built on the host) fixed values, cell
+    flags, static alpha and face weights."""
     n = sc.n
     N, NF = n ** 3, (n + 1) * n * n
+    if setup == "device":
+        return 4 * N
     return 4 * N + 4 * N + N + 4 * N + 2 * 3 * 4 * NF
 
 

@@ -60,6 +60,8 @@ class SceneSpec:
     t_max: float = 300.0
     t_init_grid: float | None = None         # initial grid temperature (default t_amb)
     defect_correction: bool = False          # fp64 true-residual check and restart after each CG solve (not in the reference)
+    statics: object = None                   # voxelize.SceneStatics built on the device: replaces fixed, tfix, source and
+                                             # the static_* arrays
     extra: dict = field(default_factory=dict)
 
 
@@ -86,8 +88,11 @@ class DeviceScene:
         self.ayc, self.azc, self.hkzc = z(n, n, n), z(n, n, n), z(n, n, n)
         self.cell_flags = z(n, n, n, dtype=torch.uint8)
         coupled = spec.n_particles > 0
-        has_static = spec.static_alpha is not None
-        if has_static:
+        dst = spec.statics
+        has_static = spec.static_alpha is not None or dst is not None
+        if dst is not None:
+            self.st_alpha, self.st_k, self.st_m = dst.alpha, list(dst.k), list(dst.m)
+        elif has_static:
             up = lambda a: torch.as_tensor(np.require(a, np.float32, ("C", "W")), device=dev)   # host copy if read-only
             self.st_alpha = up(spec.static_alpha)
             self.st_k = [up(a) for a in spec.static_k]
@@ -123,10 +128,13 @@ class DeviceScene:
         self.state = torch.frombuffer(bytearray(bytes(st0)), dtype=torch.uint8).to(dev)
         self._parity_host = 0
         self.dirty = False
-        fixed = np.zeros((n, n, n), bool) if spec.fixed is None else np.asarray(spec.fixed, bool)
-        tfix = np.zeros((n, n, n), np.float32) if spec.tfix is None else spec.tfix
-        source = np.zeros((n, n, n), bool) if spec.source is None else np.asarray(spec.source, bool)
-        self._set_flags(fixed, tfix, source)
+        if dst is not None:
+            self.cell_flags, self.tfix = dst.cell_flags, dst.tfix
+        else:
+            fixed = np.zeros((n, n, n), bool) if spec.fixed is None else np.asarray(spec.fixed, bool)
+            tfix = np.zeros((n, n, n), np.float32) if spec.tfix is None else spec.tfix
+            source = np.zeros((n, n, n), bool) if spec.source is None else np.asarray(spec.source, bool)
+            self._set_flags(fixed, tfix, source)
         self.rate, self.t_cap = float(spec.rate), float(spec.t_cap)
         self.record = _lib.Scene()
         self.fill_record()

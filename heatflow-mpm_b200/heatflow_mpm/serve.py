@@ -55,7 +55,7 @@ def poisson_trace(rate=20.0, duration=60.0, seed=0, edges=(48, 64, 96, 128), hor
 
 class AirServer:
     def __init__(self, device="cuda:0", dt=2e-3, hbm_budget=150e9, max_slots=256, persistent_blocks=0, group_cells=0,
-                 lanes=0, keep_results=False, result_fields=("T",)):
+                 lanes=0, keep_results=False, result_fields=("T",), setup="device"):
         self.device = torch.device(device)
         self.dt = dt
         self.budget = float(hbm_budget)
@@ -65,6 +65,8 @@ class AirServer:
         self.lanes = lanes
         self.keep_results = keep_results
         self.result_fields = ("T", "u", "v", "w") if keep_results else tuple(result_fields)
+        self.setup = setup               # scene statics built on the device ("device") or on the host ("host")
+        self.admit_ms: list[float] = []  # host time of building each admitted scene (statics, upload, face fractions)
         self.h2d_bytes = 0
         self.d2h_bytes = 0
         self.queue = collections.deque()
@@ -89,10 +91,12 @@ class AirServer:
             if self.used + need > self.budget:
                 break
             self.queue.popleft()
-            req.scene = make_scene(req.scenario, self.device)
-            self.h2d_bytes += upload_bytes(req.scenario)
+            t0 = time.perf_counter()
+            req.scene = make_scene(req.scenario, self.device, setup=self.setup)
+            self.h2d_bytes += upload_bytes(req.scenario, self.setup)
             # the new scene's static obstacle fields, face fractions and conductivity, prepared on its own
             ScenePlan([req.scene], self.device).prepare_statics()
+            self.admit_ms.append(1e3 * (time.perf_counter() - t0))
             req.admitted = now
             self.used += need
             self.active.append(req)
@@ -179,4 +183,5 @@ class AirServer:
                 "substeps96_per_s": self.weighted_substeps / el,
                 "request_latency_p50_s": q(lat, 50), "request_latency_p99_s": q(lat, 99),
                 "substep_latency_p50_ms": q(self.substep_ms, 50), "substep_latency_p99_ms": q(self.substep_ms, 99),
-                "batched_substeps": len(self.substep_ms), "plan_builds": self.plan_builds, "elapsed_s": el}
+                "batched_substeps": len(self.substep_ms), "plan_builds": self.plan_builds, "elapsed_s": el,
+                "setup": self.setup, "admit_ms_p50": q(self.admit_ms, 50), "admit_ms_p99": q(self.admit_ms, 99)}

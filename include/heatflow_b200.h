@@ -211,6 +211,59 @@ int hf_k_laplacian(int n, double h, double alpha, double beta, const float *p, c
 int hf_k_heat_matvec(int n, double h, double dt, double alpha, double beta, const float *x, const float *kap,
                      const uint8_t *cell_flags, const float *y, float *out, void *stream);
 
+/* ------------------------------------------------------------------------------------ scene set-up on the device */
+/* Geometry of one scene's heater and optional static sphere.  The host fills it from the heater's parameters: the
+ * frame of heater.py:24-31 (Heater.frame) and the thresholds of heater.py:42-49, each evaluated by the expression
+ * heater.py writes (e.g. shell_out = R + 0.006 + h / 2), so that the device compares against the same binary64 values. */
+typedef struct hf_heater_geometry {
+    int32_t kind;            /* 0: no heater (off), 1: the trough heater of heater.py:33-49, 2: a box heater block */
+    int32_t fan;             /* 1 when the fan runs (fan > 0): fan outlet cells and fan faces */
+    double centre[3], facing[3], axis[3], up[3];   /* trough frame (heater.py:24-31) */
+    double half_length;      /* L2 = length / 2 */
+    double shell_in;         /* R - h / 2 */
+    double shell_out;        /* R + 0.006 + h / 2 */
+    double cap_half;         /* h / 2 */
+    double cap_radius;       /* R + 0.006 */
+    double rod_half;         /* L2 - 0.015 */
+    double rod_radius;       /* 0.007 + h / 2 */
+    double rod_front;        /* 0.03: rods at q = -0.03 */
+    double rod_dz;           /* 0.03: rods at r = -0.03 and r = +0.03 */
+    double fan_half;         /* L2 - 0.02 */
+    double fan_high;         /* R - 0.01 */
+    double fan_depth;        /* 0.015 */
+    double trough_half;      /* L2 - 0.015 */
+    double trough_radius;    /* R - 0.004 */
+    int32_t box_lo[3], box_hi[3];   /* box heater: rods in i in [lo0, hi0), j in [lo1, hi1), k in [0, hi2) */
+    int32_t box_trough;      /* box heater: the trough-air layer k (the fan layer is k + 1) */
+    int32_t sphere;          /* 1: a static solid sphere */
+    double t_rod, t_amb;     /* Dirichlet values of rods and walls */
+    float m_face[3];         /* momentum weight of a fan face per axis: float32(K_FAN * fan * facing[axis]) */
+    float k_solid, k_fan;    /* K_SOLID and K_FAN as float32 (heater.py:7) */
+    float sphere_t;          /* the sphere's cells are fixed at this temperature */
+    int32_t sphere_lo, sphere_hi, sphere_top;   /* sphere cells lie in i, j in [lo, hi), k in [0, top) */
+    int32_t pad_;
+    double sphere_c, sphere_zc, sphere_rr;      /* centre (c, c, zc) and squared radius */
+} hf_heater_geometry;
+
+/* heater.py:33-65 Heater.masks and solver.py:48-56 on the device, for one scene of edge n and cell size h:
+ *   cell_class (n^3 bytes): the heater's cell type (0 air, 1 shell, 2 rod, 3 fan, 4 trough air), + 8 on sphere cells;
+ *   cell_flags (n^3 bytes): bit0 fixed (rods, side walls and ceiling, sphere), bit1 source (fan and trough air);
+ *   tfix (n^3 floats): rods t_rod, walls t_amb, sphere sphere_t (sphere before rods before walls), 0 elsewhere;
+ *   alpha (n^3 floats): static solid fraction, 1 on shell, rod and sphere cells;
+ *   kx, ky, kz / mx, my, mz (face lattices): static relaxation and momentum weights (heater.py:53-63; sphere faces
+ *   K_SOLID toward rest).
+ * counts (device, 2 ints, cleared by the call): [0] source cells (the host forms heater.py:52's rate from it),
+ * [1] cells whose class depends on a comparison closer than 1e-12 m to its threshold (0 means the classes do not
+ * depend on the host CPU's floating-point evaluation order). */
+int hf_scene_statics(const hf_heater_geometry *geometry, int n, double h, uint8_t *cell_class, uint8_t *cell_flags,
+                     float *tfix, float *alpha, float *kx, float *ky, float *kz, float *mx, float *my, float *mz,
+                     int32_t *counts, void *stream);
+/* shapes.py:13-17 _inside (Warp's mesh_query_point_sign_winding_number): generalized winding number of each of
+ * num_points points (x, y, z float32) against a triangle soup (num_tri x 9 floats: v0, v1, v2); flag[i] = 1 when it
+ * exceeds threshold (0.5: inside); winding (optional) receives the numbers themselves.  Exact sum over all triangles. */
+int hf_winding_inside(const float *tri, int num_tri, const float *points, int num_points, float threshold,
+                      int32_t *flag, float *winding, void *stream);
+
 /* ------------------------------------------------------------------------------------ without device allocation */
 /* No counterpart in the reference: an entry point for callers that cannot allocate device memory (code running where
  * no allocator may be called -- inside an allocator callback, under a memory budget owned by someone else, or in a

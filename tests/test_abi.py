@@ -51,14 +51,16 @@ def test_record_layout_matches_header(tmp_path):
         pytest.skip("gcc unavailable")
     from heatflow_mpm import _lib
     prog = tmp_path / "sizes.c"
-    prog.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\nint main(){printf("%%zu %%zu %%zu %%zu %%zu %%zu\\n",'
-                    'sizeof(hf_scene),sizeof(hf_plan),sizeof(hf_scene_state),offsetof(hf_scene,T),offsetof(hf_scene,state),'
-                    'offsetof(hf_scene_state,rhs_mean));return 0;}\n' % HEADER)
+    prog.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\nint main(){printf("%%zu %%zu %%zu %%zu %%zu %%zu '
+                    '%%zu %%zu %%zu\\n",sizeof(hf_scene),sizeof(hf_plan),sizeof(hf_scene_state),offsetof(hf_scene,T),'
+                    'offsetof(hf_scene,state),offsetof(hf_scene_state,rhs_mean),sizeof(hf_heater_geometry),'
+                    'offsetof(hf_heater_geometry,m_face),offsetof(hf_heater_geometry,sphere_c));return 0;}\n' % HEADER)
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", str(prog), "-o", str(exe)], check=True)
     got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
     want = [C.sizeof(_lib.Scene), C.sizeof(_lib.Plan), C.sizeof(_lib.SceneState), _lib.Scene.T.offset,
-            _lib.Scene.state.offset, _lib.SceneState.rhs_mean.offset]
+            _lib.Scene.state.offset, _lib.SceneState.rhs_mean.offset, C.sizeof(_lib.HeaterGeometry),
+            _lib.HeaterGeometry.m_face.offset, _lib.HeaterGeometry.sphere_c.offset]
     assert [int(x) for x in got] == want
 
 

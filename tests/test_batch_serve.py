@@ -78,7 +78,7 @@ def test_admission_respects_slots_and_hbm_budget(monkeypatch):
         def prepare_statics(self):
             pass
 
-    monkeypatch.setattr(serve, "make_scene", lambda sc, dev: object())
+    monkeypatch.setattr(serve, "make_scene", lambda sc, dev, **kw: object())
     monkeypatch.setattr(serve, "ScenePlan", FakePlan)
 
     class Server(serve.AirServer):
