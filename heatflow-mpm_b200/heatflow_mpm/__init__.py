@@ -7,5 +7,6 @@ from .solver import HeatflowMPM, KAPPA_AIR  # noqa: F401
 from .batch import AirScenario, AirBatch, autotune, ensemble, shard_scenarios  # noqa: F401
 from .serve import AirServer, Request, poisson_trace  # noqa: F401
 from .frames import FrameWriter  # noqa: F401
+from .shapes import load_mesh, sample_interior, mesh_particles, BUNNY  # noqa: F401
 
 __version__ = "0.3.0"

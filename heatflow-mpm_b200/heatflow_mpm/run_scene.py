@@ -6,9 +6,10 @@ scripts/run_scene.py:14-44 on this package: same arguments, defaults and output 
 Output: static.npz, meta.json, frames/frame_NNNN.npz (pos, vel, temp f16, melt f16, grid_T f16 [n^3], air_u f16
 [n^3, 3]).  Frames are packed on the device and written by FrameWriter while the substeps continue.
 
-The body: ``--mesh ellipsoid`` (default) fills the 4/3/5 cm ellipsoid scaled to ``--height``; a ``.npy`` file is taken
-as particle positions.  Mesh files need the mesh loader and winding-number fill of the reference (trimesh), which
-this package does not carry.  The material solver is Newton's implicit MPM when it is installed, otherwise
+The body: ``--mesh`` names a Wavefront OBJ file, filled as shapes.py:47-51 fills it (jittered lattice, inside test by
+the generalized winding number on the GPU); the default is the reference's bunny when $HEATFLOW_ASSETS/bunny.obj
+exists (the mesh is not shipped), otherwise ``ellipsoid``: the 4/3/5 cm ellipsoid scaled to ``--height``.  A ``.npy``
+file is taken as particle positions.  The material solver is Newton's implicit MPM when it is installed, otherwise
 ``--body frozen`` keeps the particles in place.
 """
 from __future__ import annotations
@@ -34,8 +35,15 @@ def body_particles(a) -> np.ndarray:
         return P
     if a.mesh.endswith(".npy"):
         return np.load(a.mesh).astype(np.float32)
-    raise SystemExit(f"--mesh {a.mesh}: mesh files need a mesh loader (trimesh) that is not installed; "
-                     "use --mesh ellipsoid or a .npy file of particle positions")
+    if not os.path.exists(a.mesh):
+        raise SystemExit(f"--mesh {a.mesh}: no such file (give an OBJ mesh, a .npy of particle positions or 'ellipsoid')")
+    from .shapes import mesh_particles
+    return mesh_particles(a.mesh, a.height, a.spacing, a.L, a.seed, a.yaw, a.device)
+
+
+def _default_mesh() -> str:
+    from .shapes import BUNNY
+    return BUNNY if os.path.exists(BUNNY) else "ellipsoid"
 
 
 def parse(argv=None):
@@ -44,7 +52,7 @@ def parse(argv=None):
     ap.add_argument("--seconds", type=float, default=20.0)
     ap.add_argument("--frame-dt", type=float, default=0.02)
     ap.add_argument("--dt", type=float, default=2e-3)
-    ap.add_argument("--mesh", default="ellipsoid")
+    ap.add_argument("--mesh", default=_default_mesh())
     ap.add_argument("--height", type=float, default=0.10)
     ap.add_argument("--yaw", type=float, default=0.0)
     ap.add_argument("--seed", type=int, default=0)

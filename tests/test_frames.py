@@ -9,14 +9,31 @@ import pytest
 
 def test_cli_body_and_mesh_refusal():
     from heatflow_mpm.run_scene import body_particles, parse
-    a = parse(["--out", "x"])
+    a = parse(["--out", "x", "--mesh", "ellipsoid"])
     assert (a.seconds, a.frame_dt, a.dt, a.h, a.L, a.power, a.t_cap, a.t_sol, a.t_liq) == \
            (20.0, 0.02, 2e-3, 0.005, 0.48, 400.0, 120.0, 30.0, 36.0)
     P = body_particles(a)
     assert P.dtype == np.float32 and 10_000 < len(P) < 25_000 and P[:, 2].min() >= 0.0
-    a2 = parse(["--out", "x", "--mesh", "bunny.obj"])
+    a2 = parse(["--out", "x", "--mesh", "no_such_mesh.obj"])
     with pytest.raises(SystemExit):
         body_particles(a2)
+
+
+@pytest.mark.gpu
+def test_cli_fills_obj_mesh(tmp_path):
+    """--mesh file.obj: the body is shapes.py's mesh_particles of that file with the CLI's height, spacing, box, seed
+    and yaw."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    from heatflow_mpm.run_scene import body_particles, parse
+    from heatflow_mpm.shapes import mesh_particles
+    from test_scene_setup import torus, write_obj
+    p = tmp_path / "t.obj"
+    write_obj(p, *torus())
+    a = parse(["--out", "x", "--mesh", str(p), "--height", "0.05", "--yaw", "20", "--seed", "4"])
+    P = body_particles(a)
+    assert len(P) > 1000 and np.array_equal(P, mesh_particles(str(p), 0.05, 2.5e-3, 0.48, 4, 20.0))
 
 
 def _same(a, b):
