@@ -527,7 +527,6 @@ def bench_batched(args, dev, rank, world, local, steps, warmup, cpu_sample=True)
             state_h[i].copy_(s.state, non_blocking=True)
         torch.cuda.synchronize()
     e2e_s = reduce_max(time.perf_counter() - t0, dev, world)
-    st_e1 = sc.read_state()
     e2e = {"value": cells * e2e_steps / N96 / e2e_s, "unit": "96^3-equivalent substeps/s", "h2d_bytes_per_step": 0,
            "d2h_bytes_per_step": int(state_h.numel()), "steps": e2e_steps,
            "note": "AirBatch.substep (eager, no graph) + every scene's state block copied to pinned host memory"}
