@@ -3,7 +3,8 @@
 Same constructor, methods and attributes as the reference.  One extra keyword, ``body``, chooses the material solver:
 ``"newton"`` (default: Newton's SolverImplicitMPM, as the reference) or ``"frozen"`` (particles keep their positions
 and velocities; used when Newton is not installed).  The air substep itself -- obstacle fields, temperature stages,
-heat CG, FLIP particle update, face stage, pressure CG and projection -- is one call into libheatflow_b200."""
+heat CG, FLIP particle update, face stage, pressure CG and projection -- is one call into libheatflow_b200, replayed
+from a CUDA graph after the first substep at each dt (``graph=False``: launched directly every time; same bits)."""
 from __future__ import annotations
 
 from dataclasses import asdict
@@ -56,10 +57,13 @@ class HeatflowMPM:
     def __init__(self, particles: np.ndarray, mat: Material = Material(), heater: Heater = Heater(),
                  grid: GridConfig = GridConfig(), spacing: float = 2.5e-3, t_init: float = 20.0,
                  kappa_air: float = KAPPA_AIR, device: str = "cuda:0", *, body: str = "newton",
-                 particle_velocities=None, heat_tol: float = 1e-6, heat_maxiter: int = 200, persistent_blocks: int = 0):
+                 particle_velocities=None, heat_tol: float = 1e-6, heat_maxiter: int = 200, persistent_blocks: int = 0,
+                 graph: bool = True):
         if not torch.cuda.is_available():
             raise RuntimeError("HeatflowMPM needs a CUDA device (sm_100a); there is no CPU path")
         self.mat, self.heater, self.dev, self.spacing, self.kappa_air = mat, heater, device, spacing, kappa_air
+        self.use_graph = bool(graph)
+        self._graph, self._graph_key = None, None
         self.grid = AirGrid(grid, device)
         self.heat = HeatField(self.grid.n, self.grid.h, grid.t_amb, device)
         particles = np.zeros((0, 3), np.float32) if particles is None else np.asarray(particles, np.float32)
@@ -94,13 +98,44 @@ class HeatflowMPM:
                 pos, vel = b.particle_state()
                 sc.pos.copy_(pos)
                 sc.pvel.copy_(vel)
-            self.plan.substep(dt)
+            self._air_substep(dt)
             if b is not None:
                 ys, vs = b.material_outputs()
                 if ys.data_ptr() != sc.pyield.data_ptr():
                     ys.copy_(sc.pyield)
                     vs.copy_(sc.pvisc)
                 b.step(dt)
+
+    def _air_substep(self, dt: float):
+        """The air substep's launches.  With graph=True the first substep at a given dt (and plan options) runs eagerly
+        and is then recorded as a CUDA graph that later substeps replay: the same launches, bit for bit, without the
+        host in the loop (the kernels read the buffer parity on the device, so one recording serves every substep).
+        A changed scene record (set_source) is uploaded first and drops the recording; inside a caller's own stream
+        capture the launches are issued directly."""
+        plan = self.plan
+        if not self.use_graph or torch.cuda.is_current_stream_capturing():
+            plan.substep(dt)
+            return
+        if any(sc.dirty for sc in plan.scenes):
+            plan.upload()
+            for sc in plan.scenes:
+                sc.dirty = False
+            self._graph = None
+        key = (float(dt), int(plan.plan.options), int(plan.plan.persistent_blocks), int(plan.plan.group_cells))
+        if self._graph is not None and self._graph_key == key:
+            self._graph.replay()
+            return
+        plan.substep(dt)
+        dev = torch.device(self.dev)
+        cur = torch.cuda.current_stream(dev)
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(cur)
+        g = torch.cuda.CUDAGraph()
+        # thread-local capture: a frame writer's thread may wait on its own copies meanwhile
+        with torch.cuda.graph(g, stream=side, capture_error_mode="thread_local"):
+            plan.substep(dt)
+        cur.wait_stream(side)
+        self._graph, self._graph_key = g, key
 
     def status(self) -> dict:
         """Solver status of the last substep: CG iterations, residuals, status bits (0 = converged everywhere)."""
