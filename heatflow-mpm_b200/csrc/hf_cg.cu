@@ -79,7 +79,21 @@ __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b
 #pragma unroll
     for (int q = 0; q < K; ++q) tot[q] = 0.0;
     if (threadIdx.x < kThreads) {
-        for (int c = b + threadIdx.x; c < e; c += kThreads) {
+        // a thread's partials c = b + t, b + t + 256, ... are added in that order; four are loaded before they are
+        // added, so their L2 round trips overlap instead of each waiting for the previous addition
+        int c = b + threadIdx.x;
+        for (; c + 3 * kThreads < e; c += 4 * kThreads) {
+            double v[4][K];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int q = 0; q < K; ++q) v[u][q] = buf[STRIDE * (c + u * kThreads) + comp[q]];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int q = 0; q < K; ++q) tot[q] += v[u][q];
+        }
+        for (; c < e; c += kThreads) {
 #pragma unroll
             for (int q = 0; q < K; ++q) tot[q] += buf[STRIDE * c + comp[q]];
         }
