@@ -605,6 +605,8 @@ def bench_served(args, dev, rank, world, local, cpu_sample=True):
                        "substep_latency_p50_ms": out["substep_latency_p50_ms"],
                        "substep_latency_p99_ms": out["substep_latency_p99_ms"],
                        "scene_substeps": int(scene_substeps), "plan_builds": out["plan_builds"],
+                       "scene_setup": out["setup"], "admit_ms_p50": out["admit_ms_p50"],
+                       "admit_ms_p99": out["admit_ms_p99"],
                        "gpu_busy_frac": busy_s / wall_s, "parallelism": f"request-sharded x{world}",
                        "latency_note": "request latency = arrival to last substep, over completed requests (rank 0)",
                        "l2": "resident scene state of the admitted requests >> 126 MB L2"},
