@@ -445,6 +445,58 @@ def bench_plain(args, dev, rank, world, local):
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * steps, "clocks": ck}
 
 
+# ---------------------------------------------------------------------------------------------------- config 1
+CONFIG1 = ("32^3 air-only plume: h=15 mm, box heater (4x4x2 rod cells at x=0.1 m + trough layer), 400 W capped at "
+           "120 C, fan 0, walls 25 C, seeded +-0.01 K noise, pressure and heat CG tol 1e-6, dt=2 ms, 100 substeps")
+
+
+def config1_summary(dev, cpu=True, cpu_seconds=20.0):
+    """The CPU-runnable configuration end to end: its 100 substeps on the GPU through HeatflowMPM.substep (CUDA events
+    on the stream; the 4 MB state stays in L2; timed after one untimed substep that records the substep graph, from
+    the restored initial state) and, with cpu=True, on the CPU port at one thread and at all host threads from the
+    same initial state (each bounded to cpu_seconds)."""
+    import torch
+    from heatflow_mpm.synthetic import plume_box
+    sim = plume_box(device=dev)
+    sc = sim.scene
+    T0 = sc.current("T").cpu().numpy().copy()
+    sim.substep(DT)
+    torch.cuda.synchronize()
+    for nm in ("u", "v", "w"):
+        sc.current(nm).zero_()
+    sc.set_current("T", T0)
+    sc.p.zero_()
+    st0 = sc.read_state()
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(100):
+        sim.substep(DT)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    st1 = sc.read_state()
+    out = {"workload": CONFIG1, "substeps": 100,
+           "gpu": {"value": 100 / (ms / 1000.0), "unit": "substeps/s", "ms_per_step": ms / 100,
+                   "mean_pressure_iters": (st1.total_pressure_iters - st0.total_pressure_iters) / 100,
+                   "mean_heat_iters": (st1.total_heat_iters - st0.total_heat_iters) / 100, "status": int(st1.status)}}
+    if cpu:
+        from oracle import oracle as O
+        res = {}
+        for label, threads in (("threads_1", 1), ("threads_all", host_threads())):
+            O.set_threads(threads)
+            osc = O.scene_from_spec(sc.spec, "f32", mean_mode=0, scatter_mode=0)
+            osc.set_state(T=T0)
+            done, el = time_cpu_substeps(osc, cpu_seconds, max_steps=100)
+            res[label] = {"value": done / el, "unit": "substeps/s", "threads": O.num_threads(), "substeps": done,
+                          "seconds": el}
+        O.set_threads(host_threads())
+        out["cpu_port"] = dict(res, kind="port", sample="the same substeps from the same initial state on the CPU "
+                                                          "port (oracle/hf_oracle.c, OpenMP)")
+    return out
+
+
 # --------------------------------------------------------------------------------------------------- batched
 def bench_batched(args, dev, rank, world, local, steps, warmup, cpu_sample=True):
     import torch
@@ -642,6 +694,8 @@ def main():
     if args.workload == "plain":
         out = bench_plain(args, dev, rank, world, local)
         if not args.no_extras:
+            if rank == 0 and world == 1:
+                out["config1"] = config1_summary(dev, cpu=not args.no_cpu_baseline, cpu_seconds=args.cpu_seconds)
             b = bench_batched(args, dev, rank, world, local, steps=200, warmup=3, cpu_sample=False)
             out["batched"] = compact(b)
             out["batched"]["plain_ratio"] = b["value"] / out["value"]

@@ -193,3 +193,26 @@ def test_resident_cg_matches_streaming_cg(torch_cuda, n):
         assert np.array_equal(a.p.cpu().numpy(), b.p.cpu().numpy())
         sb = b.read_state()
         assert (sa.pressure_iters, sa.heat_iters, sa.status) == (sb.pressure_iters, sb.heat_iters, sb.status)
+
+
+def test_config1_air_only_plume_100_substeps(torch_cuda):
+    """The CPU-runnable configuration end to end: 32^3 air-only plume (h = 15 mm, box heater of 4x4x2 rod cells at
+    x = 0.1 m with its trough layer, 400 W capped at 120 C, fan 0), seeded +-0.01 K noise, pressure and heat CG tol
+    1e-6, 100 substeps through HeatflowMPM.substep against the oracle in the build's arithmetic: T, u, v, w within
+    relative L2 1e-6 every 20 substeps; every solve converged; the plume rises above the heater."""
+    from heatflow_mpm.synthetic import plume_box
+    sim = plume_box()
+    sc = sim.scene
+    orc = oracle_from_spec(sc.spec)
+    orc.set_state(T=sc.current("T").cpu().numpy())
+    for s in range(1, 101):
+        sim.substep(2e-3)
+        orc.substep(2e-3)
+        assert sc.read_state().status == 0, s
+        if s % 20 == 0:
+            for nm in ("T", "u", "v", "w"):
+                assert rel_l2(sc.current(nm).cpu().numpy(), getattr(orc, nm)) <= 1e-6, (nm, s)
+    w = sc.current("w").cpu().numpy()
+    i0, j0 = int(round(0.10 / sim.grid.h)) - 2, sim.grid.n // 2 - 2
+    assert w[i0:i0 + 4, j0:j0 + 4, 4:10].mean() > 1e-3              # warm air rising above the block
+    assert sim.grid.divergence_max() < 1e-3
