@@ -520,8 +520,7 @@ def bench_batched(args, dev, rank, world, local, steps, warmup, cpu_sample=True)
     batch.capture(DT, G)
     torch.cuda.synchronize()
     st0 = batch.states()
-    # the fields a substep starts from (the end-to-end leg below repeats the timed substeps from here)
-    start = [dict({nm: sc.current(nm).clone() for nm in ("T", "u", "v", "w")}, p=sc.p.clone()) for sc in batch.scenes]
+    start = batch.snapshot()   # the end-to-end leg below repeats the timed substeps from here
     stream = torch.cuda.current_stream()
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
@@ -571,10 +570,7 @@ def bench_batched(args, dev, rank, world, local, steps, warmup, cpu_sample=True)
     sub_gbs = sb / (el_ms / steps / 1000.0) / 1e9
     # ---- end to end through the public API: AirBatch.substep per substep, every scene's status block read back
     state_h = torch.empty((len(batch.scenes), batch.scenes[0].state.numel()), dtype=torch.uint8).pin_memory()
-    for sc, st in zip(batch.scenes, start):
-        for nm in ("T", "u", "v", "w"):
-            sc.current(nm).copy_(st[nm])
-        sc.p.copy_(st["p"])
+    batch.restore(start)
     del start
     e2e_steps = steps
     barrier(world)

@@ -185,6 +185,18 @@ class AirBatch:
     def states(self):
         return [sc.read_state() for sc in self.scenes]
 
+    def snapshot(self):
+        """Device copies of what the next substep starts from in every scene: the current T, u, v, w and the pressure
+        (the CG warm start).  Air-only scenes carry no other state from one substep to the next."""
+        return [dict({nm: sc.current(nm).clone() for nm in ("T", "u", "v", "w")}, p=sc.p.clone()) for sc in self.scenes]
+
+    def restore(self, snap):
+        """Put a snapshot back: the substeps that follow compute the same bits as they did after it was taken."""
+        for sc, st in zip(self.scenes, snap):
+            for nm in ("T", "u", "v", "w"):
+                sc.current(nm).copy_(st[nm])
+            sc.p.copy_(st["p"])
+
 
 # ---------------------------------------------------------------------------------------------------- autotuner
 _CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotune_cache.json")
@@ -199,7 +211,9 @@ def _signature(scenes):
 
 def autotune(batch: AirBatch, dt=2e-3, reps=3, candidates=None, cache=True):
     """Time launch-shape candidates (persistent_blocks, group_cells, lanes) of the CG solves on this batch and keep
-    the fastest.  Returns (the chosen triple, {"blocks/cells/lanes": ms per substep})."""
+    the fastest.  Every candidate times the same `reps` substeps from the batch's current state (restored before each
+    one, after a warm-up substep), and the batch is left as it was found.  Returns (the chosen triple,
+    {"blocks/cells/lanes": ms per substep})."""
     sms = torch.cuda.get_device_properties(batch.device).multi_processor_count
     name = torch.cuda.get_device_name(batch.device)
     key = f"{name}|{_signature(batch.scenes)}"
@@ -214,12 +228,14 @@ def autotune(batch: AirBatch, dt=2e-3, reps=3, candidates=None, cache=True):
         best = tuple(int(v) for v in table[key]["choice"])
         plan.plan.persistent_blocks, plan.plan.group_cells, plan.lanes = best
         return best, table[key]["timings"]
-    candidates = candidates or [(b * sms, g, l) for (g, l) in ((1, 1), (1, 2), (0, 1), (0, 2), (1, 4), (0, 4))
+    candidates = candidates or [(b * sms, g, l) for (g, l) in ((1, 1), (1, 2), (0, 1), (0, 2), (1, 4), (0, 4), (0, 8))
                                 for b in (2, 4, 5)]
     timings = {}
+    snap = batch.snapshot()
     for pb, gc, ln in candidates:
         plan.plan.persistent_blocks, plan.plan.group_cells, plan.lanes = pb, gc, ln
         batch.plan.substep(dt)                       # warm-up
+        batch.restore(snap)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         for _ in range(reps):
@@ -227,6 +243,8 @@ def autotune(batch: AirBatch, dt=2e-3, reps=3, candidates=None, cache=True):
         b.record()
         torch.cuda.synchronize()
         timings[(pb, gc, ln)] = a.elapsed_time(b) / reps
+        batch.restore(snap)
+    del snap
     best = min(timings, key=timings.get)
     plan.plan.persistent_blocks, plan.plan.group_cells, plan.lanes = best
     out = {"/".join(str(v) for v in k): t for k, t in timings.items()}

@@ -200,19 +200,26 @@ def test_served_scenes_match_alone(cuda):
 
 @pytest.mark.gpu
 def test_autotune_keeps_results(cuda):
-    """Every launch shape (blocks, group size, lanes) computes the same bits: a tuned batch ends where an untuned one
-    does."""
+    """Tuning leaves the batch where it was, and every launch shape (blocks, group size, lanes) computes the same
+    bits: two substeps under each candidate, from the restored start, equal two substeps of an untuned batch."""
     from heatflow_mpm.batch import AirBatch, autotune
     scs = _scenarios()
     b = AirBatch(scs)
     sms = cuda.cuda.get_device_properties(0).multi_processor_count
-    cands = [(2 * sms, 1, 4), (4 * sms, 0, 1), (sms, 20_000, 2), (3 * sms, 1, 3)]
-    best, timings = autotune(b, reps=1, candidates=cands, cache=False)
-    assert best in cands and len(timings) == 4
+    cands = [(2 * sms, 1, 4), (4 * sms, 0, 1), (sms, 20_000, 2), (3 * sms, 1, 3), (2 * sms, 0, 8)]
     ref = AirBatch(scs)
-    for _ in range(4 * (1 + 1)):                        # autotune ran 4 candidates x (1 warm-up + reps)
+    same = lambda x, y: all(np.array_equal(a.current(nm).cpu().numpy(), c.current(nm).cpu().numpy())
+                            for a, c in zip(x.scenes, y.scenes) for nm in ("T", "u", "v", "w"))
+    best, timings = autotune(b, reps=1, candidates=cands, cache=False)
+    assert best in cands and len(timings) == len(cands)
+    assert same(b, ref)
+    start = b.snapshot()
+    for _ in range(2):
         ref.substep(2e-3)
-    for a, c in zip(b.scenes, ref.scenes):
-        for nm in ("T", "u", "v", "w"):
-            assert np.array_equal(a.current(nm).cpu().numpy(), c.current(nm).cpu().numpy()), nm
-        assert a.read_state().pressure_iters == c.read_state().pressure_iters
+    for pb, gc, ln in cands:
+        b.restore(start)
+        b.plan.plan.persistent_blocks, b.plan.plan.group_cells, b.plan.lanes = pb, gc, ln
+        for _ in range(2):
+            b.substep(2e-3)
+        assert same(b, ref), (pb, gc, ln)
+        assert [s.read_state().pressure_iters for s in b.scenes] == [s.read_state().pressure_iters for s in ref.scenes]
