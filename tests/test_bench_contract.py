@@ -65,24 +65,59 @@ def _bound(nodes, into_functions):
     return out
 
 
-def _unbound_reads(fn, visible, found):
-    local = _bound(list(ast.iter_child_nodes(fn)), False) | visible
-    stack = list(ast.iter_child_nodes(fn))
+def _reads(nodes, visible, where, found):
+    """Names read by `nodes` (evaluated in a scope that sees `visible`) that nothing binds."""
+    stack = list(nodes)
     while stack:
         n = stack.pop()
-        if isinstance(n, (ast.FunctionDef, ast.AsyncFunctionDef)):
-            _unbound_reads(n, local, found)
+        if isinstance(n, (ast.FunctionDef, ast.AsyncFunctionDef, ast.Lambda)):
+            _unbound_reads(n, visible, found)      # its decorators and defaults are read here, its body in its own scope
             continue
-        if isinstance(n, ast.Name) and isinstance(n.ctx, ast.Load) and n.id not in local:
-            found.append(f"{fn.name}:{n.lineno}: {n.id}")
+        if isinstance(n, ast.ClassDef):
+            _reads(n.decorator_list + n.bases, visible, where, found)
+            inside = visible | _bound(n.body, False)       # class-body names: seen by the body's own statements and by
+            for st in n.body:                              # method decorators and defaults, not by method bodies
+                if isinstance(st, (ast.FunctionDef, ast.AsyncFunctionDef)):
+                    _unbound_reads(st, visible, found, outer=inside)
+                else:
+                    _reads([st], inside, n.name, found)
+            continue
+        if isinstance(n, ast.Name) and isinstance(n.ctx, ast.Load) and n.id not in visible:
+            found.append(f"{where}:{n.lineno}: {n.id}")
         stack.extend(ast.iter_child_nodes(n))
 
 
-def test_bench_functions_read_only_bound_names():
-    tree = ast.parse(open(BENCH).read())
+def _unbound_reads(fn, visible, found, outer=None):
+    """fn's decorators and defaults are read in `outer` (default: visible), its body in its own scope over `visible`."""
+    args = fn.args
+    _reads(getattr(fn, "decorator_list", []) + args.defaults + [d for d in args.kw_defaults if d is not None],
+           visible if outer is None else outer, getattr(fn, "name", "lambda"), found)
+    params = {a.arg for a in args.posonlyargs + args.args + args.kwonlyargs}
+    params |= {a.arg for a in (args.vararg, args.kwarg) if a is not None}
+    body = fn.body if isinstance(fn.body, list) else [fn.body]
+    local = _bound(body, False) | params | visible
+    _reads(body, local, getattr(fn, "name", "lambda"), found)
+
+
+def _check_file(path):
+    tree = ast.parse(open(path).read())
     module = _bound(tree.body, False) | set(dir(builtins)) | {"__file__", "__name__"}
     found = []
     for node in tree.body:
         if isinstance(node, (ast.FunctionDef, ast.AsyncFunctionDef)):
             _unbound_reads(node, module, found)
+        elif isinstance(node, ast.ClassDef):
+            _reads([node], module, node.name, found)
+    return [f"{os.path.basename(path)}:{f}" for f in found]
+
+
+def test_bench_functions_read_only_bound_names():
+    assert not _check_file(BENCH)
+
+
+def test_package_functions_read_only_bound_names():
+    import glob
+    files = glob.glob(os.path.join(ROOT, "heatflow-mpm_b200", "heatflow_mpm", "*.py"))
+    files += [os.path.join(ROOT, "__graft_entry__.py")] + glob.glob(os.path.join(ROOT, "oracle", "*.py"))
+    found = [f for p in sorted(files) for f in _check_file(p)]
     assert not found, found
