@@ -1,6 +1,7 @@
 """bench.py without a GPU: the CPU reference arm prints one JSON line with every key of the output contract (rank 0
-alone; other ranks exit 0 silently), and every name a bench.py function reads is bound somewhere it can see (a
-misspelt or stale name in a rarely taken branch would otherwise surface only on the GPU box)."""
+alone; other ranks exit 0 silently).  And for bench.py, the package, the entry module and the oracle's front end:
+every name a function reads is bound somewhere it can see (a misspelt or stale name in a branch that only a GPU run
+takes would otherwise surface only there)."""
 import ast
 import builtins
 import json
