@@ -78,7 +78,8 @@ def test_admission_respects_slots_and_hbm_budget(monkeypatch):
         def prepare_statics(self):
             pass
 
-    monkeypatch.setattr(serve, "make_scene", lambda sc, dev, **kw: object())
+    setups = []
+    monkeypatch.setattr(serve, "make_scene", lambda sc, dev, **kw: setups.append(kw.get("setup")) or object())
     monkeypatch.setattr(serve, "ScenePlan", FakePlan)
 
     class Server(serve.AirServer):
@@ -103,6 +104,11 @@ def test_admission_respects_slots_and_hbm_budget(monkeypatch):
     assert srv.scene_substeps == 3 + 3 + 2 and srv.used == 0
     s = srv.summary()
     assert s["requests_done"] == 3 and s["batched_substeps"] == 6
+    # statics built on the device by default: only the initial temperature is uploaded per admitted scene
+    from heatflow_mpm.batch import upload_bytes
+    assert setups == ["device"] * 3 and s["setup"] == "device" and s["admit_ms_p50"] is not None
+    assert srv.h2d_bytes == 2 * 4 * 96 ** 3 + 4 * 32 ** 3
+    assert upload_bytes(small, "host") > upload_bytes(small, "device") == 4 * 32 ** 3
 
 
 # ------------------------------------------------------------------------------------------------------ GPU
