@@ -53,6 +53,7 @@ PUBLISHED_SUBSTEPS_PER_S = 1000.0 / 7.0   # README.md:46 of the reference: ~7 ms
 WORKLOAD = ("default coupled scene 96^3 (h=5 mm, 400 W cap 120 C, fan 2 m/s, ~16k-particle ellipsoid, frozen body), "
             "dt=2 ms, pressure tol 1e-4, heat tol 1e-6")
 N96 = 96 ** 3
+PARITY_STEPS = 20   # plain line: substeps of the timed region replayed on the CPU port for the parity figures
 
 
 def parse():
@@ -176,6 +177,27 @@ def cpu_scenarios_sample(scenarios, budget_s, per_scene=2):
     return cells / N96 / el, done, visited, el
 
 
+def plain_config(n, spinup):
+    """`config` of the plain line, the same dict in both arms (what the workload is, not what a run measured)."""
+    return {"workload": WORKLOAD, "n": n, "cells": n ** 3, "spinup": spinup, "dt": DT,
+            "l2": "scene state ~170 MB > 126 MB L2 (inputs larger than L2); the CG working set (~35 MB) stays "
+                  "L2-resident within a substep by design"}
+
+
+def oracle_substeps(sc, steps, budget_s=None):
+    """`steps` substeps of the CPU port (fewer once budget_s seconds have passed, at least one): returns (substeps
+    done, seconds, pressure CG iterations, heat CG iterations)."""
+    t0 = time.perf_counter()
+    done, it_p, it_h = 0, 0, 0
+    while done < steps and (done == 0 or budget_s is None or time.perf_counter() - t0 < budget_s):
+        sc.substep(DT)
+        st = sc.stats()
+        it_p += int(st["grid_done"])
+        it_h += int(st["heat_done"])
+        done += 1
+    return done, time.perf_counter() - t0, it_p, it_h
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -194,7 +216,7 @@ def run_reference(args):
            "steps": done, "warmup": args.warmup, "ms_per_step": 1000.0 * el / done, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": v / PUBLISHED_SUBSTEPS_PER_S, "dtype": "f32",
            "data": "synthetic (seeded ellipsoid particles, reference heater geometry)",
-           "config": {"workload": WORKLOAD, "spinup": args.spinup, "n": spec.n, "cells": spec.n ** 3},
+           "config": plain_config(spec.n, args.spinup),
            "cpu_baseline": {"value": v, "unit": "substeps/s", "cores": O.num_threads(), "kind": "port",
                             "sample": f"{done} substeps (of --steps {steps}, bounded to {args.ref_seconds:.0f} s) of the "
                                       f"workload on the CPU port (oracle/hf_oracle.c, OpenMP), after "
@@ -377,6 +399,10 @@ def bench_plain(args, dev, rank, world, local):
     out_h = [torch.empty((n, n, n), dtype=torch.float32).pin_memory() for _ in range(2)]
     done = []
     consumed = 0.0
+    # one-time set-up of the download path (staging buffers, copy stream) and of the pinned upload, outside the timed
+    # loop; neither changes the scene state
+    sim.body.set_state(pos_h, vel_h)
+    sim.grid_T_async(out_h[1]).synchronize()
     st_e0 = sc.read_state()
     barrier(world)
     torch.cuda.synchronize()
@@ -391,6 +417,22 @@ def bench_plain(args, dev, rank, world, local):
     torch.cuda.synchronize()
     e2e_s = reduce_max(time.perf_counter() - t0, dev, world)
     st_e1 = sc.read_state()
+    # ---- parity: the first substeps of the timed region again from its start state (the same launches without the
+    # graph); the CPU port replays them below and the end states are compared
+    par_steps = min(steps, PARITY_STEPS)
+    for nm in ("T", "u", "v", "w"):
+        sc.set_current(nm, state_at_start[nm])
+    sc.p.copy_(torch.as_tensor(p_at_start, device=dev))
+    sc.ptemp.copy_(torch.as_tensor(ptemp_at_start, device=dev))
+    st_p0 = sc.read_state()
+    for _ in range(par_steps):
+        plan.substep(DT)
+    torch.cuda.synchronize()
+    st_p1 = sc.read_state()
+    gpu_end = {nm: sc.current(nm).cpu().numpy().copy() for nm in ("T", "u", "v", "w")}
+    gpu_end["ptemp"] = sc.ptemp.cpu().numpy().copy()
+    gpu_par = (int(st_p1.total_pressure_iters - st_p0.total_pressure_iters),
+               int(st_p1.total_heat_iters - st_p0.total_heat_iters), int(st_p1.status))
     e2e = {"value": world * steps / e2e_s, "unit": "substeps/s",
            "h2d_bytes_per_step": int(pos_h.numel() * 4 + vel_h.numel() * 4), "d2h_bytes_per_step": int(out_h[0].numel() * 4),
            "mean_pressure_iters": (st_e1.total_pressure_iters - st_e0.total_pressure_iters) / steps,
@@ -414,6 +456,7 @@ def bench_plain(args, dev, rank, world, local):
     sub_roof = {"bytes_per_substep": sb, "achieved": sub_gbs, "unit": "GB/s", "frac": sub_gbs / roof["peak"]}
     # ---- CPU baseline: the CPU port from the same state, bounded sample (rank 0, N = 1)
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
         O.set_threads(host_threads())
@@ -421,7 +464,12 @@ def bench_plain(args, dev, rank, world, local):
         osc.set_state(T=state_at_start["T"], u=state_at_start["u"], v=state_at_start["v"], w=state_at_start["w"])
         osc.a["p"][...] = p_at_start
         osc.a["ptemp"][: len(ptemp_at_start)] = ptemp_at_start
-        done, el = time_cpu_substeps(osc, args.cpu_seconds, max_steps=steps)
+        # the sample's first par_steps substeps are the parity replay (not time-bounded); the rest is bounded
+        done, el, o_it_p, o_it_h = oracle_substeps(osc, par_steps)
+        parity = plain_parity(gpu_end, osc, par_steps, gpu_par, (o_it_p, o_it_h))
+        if steps > par_steps and el < args.cpu_seconds:
+            d2, e2, _, _ = oracle_substeps(osc, steps - par_steps, args.cpu_seconds - el)
+            done, el = done + d2, el + e2
         threads = O.num_threads()
         # the same port on one thread, from the state the sample above reached (bounded to a third of the budget)
         O.set_threads(1)
@@ -435,14 +483,32 @@ def bench_plain(args, dev, rank, world, local):
             "warmup": args.warmup, "ms_per_step": el_ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": value / PUBLISHED_SUBSTEPS_PER_S, "dtype": "f32",
             "data": "synthetic (seeded ellipsoid particles, reference heater geometry)",
-            "config": {"workload": WORKLOAD, "n": n, "cells": N, "spinup": args.spinup, "parallelism": f"replicas x{world}",
-                       "l2": "scene state ~170 MB > 126 MB L2 (inputs larger than L2); the CG working set "
-                             "(~35 MB) stays L2-resident within a substep by design",
-                       "mean_pressure_iters": p_iters / steps, "mean_heat_iters": h_iters / steps,
-                       "cell_updates_per_s": value * N, "substep_status": int(st1.status),
-                       "substep_roofline": sub_roof, "stage_ms": stage_ms,
-                       "timed_launches": "one CUDA-graph replay of the K substeps" if use_graph else "eager launches"},
+            "config": plain_config(n, args.spinup),
+            "details": {"parallelism": f"replicas x{world}",
+                        "mean_pressure_iters": p_iters / steps, "mean_heat_iters": h_iters / steps,
+                        "cell_updates_per_s": value * N, "substep_status": int(st1.status),
+                        "substep_roofline": sub_roof, "stage_ms": stage_ms,
+                        "timed_launches": "one CUDA-graph replay of the K substeps" if use_graph else "eager launches"},
+            "parity": parity,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * steps, "clocks": ck}
+
+
+def plain_parity(gpu_end, osc, steps, gpu_iters, oracle_iters):
+    """The GPU's end state after the first `steps` timed substeps against the CPU port's replay of the same substeps
+    from the same start state (build arithmetic): relative L2 of T, u, v, w and the particle temperatures, max |dT|,
+    CG iterations (pressure, heat) and the GPU's status bits."""
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+    P = len(gpu_end["ptemp"])
+    return {"vs": "oracle/hf_oracle.c (CPU port, build arithmetic), the same substeps from the same start state",
+            "substeps": steps, "tolerance_rel_l2": 1e-6,
+            "rel_l2_T": rel(gpu_end["T"], osc.T), "rel_l2_u": rel(gpu_end["u"], osc.u),
+            "rel_l2_v": rel(gpu_end["v"], osc.v), "rel_l2_w": rel(gpu_end["w"], osc.w),
+            "rel_l2_ptemp": rel(gpu_end["ptemp"], osc.a["ptemp"][:P]),
+            "max_abs_T": float(np.abs(gpu_end["T"].astype(np.float64) - osc.T).max()),
+            "pressure_iters": {"gpu": gpu_iters[0], "oracle": oracle_iters[0]},
+            "heat_iters": {"gpu": gpu_iters[1], "oracle": oracle_iters[1]}, "gpu_status": gpu_iters[2]}
 
 
 # ---------------------------------------------------------------------------------------------------- config 1

@@ -11,6 +11,8 @@
 // start at zero.  Calls whose work overlaps on the GPU (different streams, or streams without ordering between them)
 // race on the array.
 #include <cstring>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <mutex>
 
 #include "hf_device.cuh"
@@ -55,20 +57,41 @@ ScratchLayout layout(int n, int C, int T) {
 }
 
 std::mutex g_mu;
-unsigned char* g_base[64] = {nullptr};
+// Address of the scratch array per device, with the context it was looked up in: a cached address belongs to one
+// context and does not survive cudaDeviceReset (or another driver-API context on the device), so the lookup is
+// repeated whenever the current context differs from the cached one.
+struct BaseCache {
+    CUcontext ctx = nullptr;
+    unsigned char* base = nullptr;
+};
+BaseCache g_base[64];
+PFN_cuCtxGetCurrent_v4000 g_ctx_current = nullptr;
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array on the current device (looked up once per device and context).
 int scratch_base(unsigned char** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HF_ERR_CUDA;
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_base[dev]) {
+    if (!g_ctx_current) {
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", reinterpret_cast<void**>(&g_ctx_current), cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !g_ctx_current)
+            return HF_ERR_CUDA;
+    }
+    // no context is current yet when the runtime has not touched this device; the lookup below creates it
+    CUcontext ctx = nullptr;
+    if (g_ctx_current(&ctx) != CUDA_SUCCESS) return HF_ERR_CUDA;
+    BaseCache& c = g_base[dev];
+    if (!c.base || !ctx || c.ctx != ctx) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) return HF_ERR_CUDA;
-        g_base[dev] = static_cast<unsigned char*>(p);
+        if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return HF_ERR_CUDA;
+        c.base = static_cast<unsigned char*>(p);
+        c.ctx = ctx;
     }
-    *out = g_base[dev];
+    *out = c.base;
     return HF_OK;
 }
 

@@ -273,7 +273,8 @@ int hf_winding_inside(const float *tri, int num_tri, const float *points, int nu
  * be NULL for zero solid flux); the scene record, work tables, CG workspace and CG vectors live in a fixed file-scope
  * device array of hf_noalloc_scratch_bytes() bytes (9 MiB) that every GPU loading the library holds until exit.
  * No cudaMalloc/cudaFree or allocating library call is made.  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress), so make it before any stream capture.  All calls on a device share the array: calls whose
+ * (cudaGetSymbolAddress), so make it before any stream capture; the address is cached per device together with the
+ * context it belongs to and looked up again after cudaDeviceReset or under another context.  All calls on a device share the array: calls whose
  * GPU work overlaps race; each call clears what must start at zero.  state_out (device, optional) receives the solve
  * statistics.  Returns HF_ERR_ARG for n > 64. */
 size_t hf_noalloc_scratch_bytes(void);

@@ -1,8 +1,8 @@
 """Generate the golden vectors in tests/golden/ from the reference Heatflow-MPM checkout itself.
 
-Run in the development container only (it reads the reference checkout, which does not travel):
+Run where a checkout of the reference exists (it is read at run time and does not travel with the tests):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <path of the Heatflow-MPM checkout>
 
 What it writes (all small, compressed .npz):
   * heater_*.npz  -- ``Heater.masks`` (heatflow_mpm/heater.py:33-65) outputs, produced by the reference module with
@@ -315,7 +315,7 @@ def make_substeps(hm, out, only=None):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of the reference Heatflow-MPM checkout")
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--only", nargs="*", default=None, help="heater | kernels | substep names")
     a = ap.parse_args()

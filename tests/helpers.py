@@ -67,3 +67,19 @@ def random_scene_inputs(n, seed, heater_kw=None, L=None, particles=0):
 def oracle_from_spec(spec, precision="f32", mean_mode=0, scatter_mode=0, particles=None, pvel=None, ptemp=None):
     from oracle import oracle as O
     return O.scene_from_spec(spec, precision, mean_mode, scatter_mode, particles, pvel, ptemp)
+
+
+def coupled_default_oracle(precision="f32"):
+    """The default coupled 96^3 scene (heatflow_mpm.synthetic.coupled_default) on the CPU oracle, in the build's
+    arithmetic (fp64 rhs mean, fixed-point particle sums): the same spec, particles, velocities and temperatures."""
+    from heatflow_mpm.grid import GridConfig
+    from heatflow_mpm.heater import Heater
+    from heatflow_mpm.mpm import Material
+    from heatflow_mpm.solver import KAPPA_AIR, build_spec
+    from heatflow_mpm.synthetic import ellipsoid_particles
+    from oracle import oracle as O
+    parts = ellipsoid_particles(seed=0)
+    spec, _, _, _ = build_spec(parts, Material(t_sol=28.0, t_liq=34.0), Heater(power=400.0, t_cap=120.0, fan=2.0),
+                               GridConfig(L=0.48, h=0.005, t_amb=25.0), 2.5e-3, 20.0, KAPPA_AIR)
+    return O.scene_from_spec(spec, precision, mean_mode=0, scatter_mode=0, particles=parts,
+                             pvel=np.zeros_like(parts), ptemp=np.full(len(parts), 20.0, np.float32))

@@ -31,6 +31,8 @@ def test_reference_arm_contract():
         assert k in d, k
     assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True and d["warmup"] == 3
     assert "workload" in d["config"]
+    # the same config dict as the GPU arm's plain line (bench.plain_config): what the workload is, nothing measured
+    assert set(d["config"]) == {"workload", "n", "cells", "spinup", "dt", "l2"}
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     e = d["e2e"]

@@ -216,3 +216,40 @@ def test_config1_air_only_plume_100_substeps(torch_cuda):
     i0, j0 = int(round(0.10 / sim.grid.h)) - 2, sim.grid.n // 2 - 2
     assert w[i0:i0 + 4, j0:j0 + 4, 4:10].mean() > 1e-3              # warm air rising above the block
     assert sim.grid.divergence_max() < 1e-3
+
+
+def test_headline_coupled96_vs_oracle(torch_cuda):
+    """The benchmark's own configuration -- the default coupled 96^3 scene (h = 5 mm, trough heater 400 W capped at
+    120 C, fan 2 m/s, ~16k-particle ellipsoid, frozen body) -- through HeatflowMPM.substep (CUDA-graph replay, the
+    TMA-staged resident CG variants, the footprint-box obstacle rebuild): 30 spin-up substeps, then 20 substeps on the
+    GPU and on the oracle from the same state.  Every substep: the same CG iteration counts (within 2 for the pressure
+    solve, 1 for heat), every solve converged (r.r <= atol^2, status 0); at the end relative L2 <= 1e-6 for T, u, v,
+    w and the particle temperatures."""
+    torch = torch_cuda
+    from heatflow_mpm.synthetic import coupled_default
+    from oracle import oracle as O
+    from helpers import coupled_default_oracle
+    import os
+    O.set_threads(len(os.sched_getaffinity(0)))
+    sim = coupled_default()
+    sc = sim.scene
+    for _ in range(30):
+        sim.substep(2e-3)
+    torch.cuda.synchronize()
+    orc = coupled_default_oracle()
+    orc.set_state(**{nm: sc.current(nm).cpu().numpy() for nm in ("T", "u", "v", "w")})
+    orc.a["p"][...] = sc.p.cpu().numpy()
+    orc.a["ptemp"][: sim.n] = sc.ptemp.cpu().numpy()
+    for s in range(20):
+        sim.substep(2e-3)
+        orc.substep(2e-3)
+        st, ost = sc.read_state(), orc.stats()
+        assert st.status == 0, (s, st.status)
+        assert abs(st.pressure_iters - ost["grid_done"]) <= 2, (s, st.pressure_iters, ost["grid_done"])
+        assert abs(st.heat_iters - ost["heat_done"]) <= 1, (s, st.heat_iters, ost["heat_done"])
+        assert st.pressure_rr <= st.pressure_atol ** 2 * (1 + 1e-12)
+        assert st.heat_rr <= st.heat_atol ** 2 * (1 + 1e-12)
+    for nm in ("T", "u", "v", "w"):
+        got = sc.current(nm).cpu().numpy()
+        assert rel_l2(got, getattr(orc, nm)) <= 1e-6, (nm, rel_l2(got, getattr(orc, nm)))
+    assert rel_l2(sc.ptemp.cpu().numpy(), orc.a["ptemp"][: sim.n]) <= 1e-6

@@ -28,14 +28,17 @@ def _bind():
     return L, _lib
 
 
-def test_no_alloc_matches_allocating_entry_point():
+@pytest.mark.parametrize("n", [32, 37, 63, 64])
+def test_no_alloc_matches_allocating_entry_point(n):
+    """n = 64 is the stated maximum (the scratch layout's largest fill); 37 and 63 give partial tiles and a partial
+    last chunk, so the tile and chunk tables written on the device are compared with hf_plan_upload's."""
     import torch
     if not torch.cuda.is_available():
         pytest.fail("GPU test needs a CUDA device")
     from heatflow_mpm.scene import DeviceScene, ScenePlan
     L, _lib = _bind()
-    n, dt = 32, 2e-3
-    spec, T0, uvw = random_scene_inputs(n, seed=77)
+    dt = 2e-3
+    spec, T0, uvw = random_scene_inputs(n, seed=77 + n)
     sc = DeviceScene(spec)
     plan = ScenePlan([sc])
     plan.prepare_statics()               # alpha_f of the static heater body
