@@ -74,6 +74,8 @@ def parse():
                     help="plain: CG solves in the streaming kernel instead of the resident one")
     ap.add_argument("--persistent-blocks", type=int, default=0, help="plain: grid of the streaming CG kernel")
     ap.add_argument("--no-tma", action="store_true", help="plain: resident pressure CG without the TMA-staged stencil")
+    ap.add_argument("--cg", default="classic", choices=["classic", "pipelined"],
+                    help="plain: pressure solve by the classic or the pipelined (one barrier per iteration) Jacobi-PCG")
     ap.add_argument("--scenes", type=int, default=64, help="batched: scenes in the ensemble")
     ap.add_argument("--graph-steps", type=int, default=10, help="batched: substeps per captured CUDA graph")
     ap.add_argument("--edges", default="32,48,64,96,128", help="batched: grid edges the ensemble draws from")
@@ -316,7 +318,7 @@ def bench_plain(args, dev, rank, world, local):
     import torch
     from heatflow_mpm.synthetic import coupled_default
     steps = args.steps if args.steps is not None else 1000
-    sim = coupled_default(device=dev)
+    sim = coupled_default(device=dev, cg=args.cg)
     sc, plan = sim.scene, sim.plan
     plan.resident_tiles = args.resident_tiles
     plan.plan.persistent_blocks = args.persistent_blocks
@@ -725,16 +727,23 @@ def bench_served(args, dev, rank, world, local, cpu_sample=True):
                                    f"{{48,64,96,128}}, horizon U(200,2000), 100-800 W, fan 0-3 m/s, sphere r U(2,6) cm "
                                    f"p=0.5, HBM budget {args.hbm_budget / 1e9:.0f} GB, max {args.max_slots} scenes/batch",
                        "requests": len(trace_all), "requests_done": int(reduce_sum(out["requests_done"], dev, world)),
+                       "requests_failed": int(reduce_sum(out["requests_failed"], dev, world)),
                        "requests_unfinished": int(reduce_sum(out["requests_unfinished"], dev, world)),
+                       "window_s": args.serve_seconds,
+                       "completed_fraction": out["completed_fraction"],
                        "request_latency_p50_s": out["request_latency_p50_s"],
                        "request_latency_p99_s": out["request_latency_p99_s"],
+                       "unfinished_age_p50_s": out["unfinished_age_p50_s"],
+                       "unfinished_age_p99_s": out["unfinished_age_p99_s"],
                        "substep_latency_p50_ms": out["substep_latency_p50_ms"],
                        "substep_latency_p99_ms": out["substep_latency_p99_ms"],
                        "scene_substeps": int(scene_substeps), "plan_builds": out["plan_builds"],
                        "scene_setup": out["setup"], "admit_ms_p50": out["admit_ms_p50"],
                        "admit_ms_p99": out["admit_ms_p99"],
                        "gpu_busy_frac": busy_s / wall_s, "parallelism": f"request-sharded x{world}",
-                       "latency_note": "request latency = arrival to last substep, over completed requests (rank 0)",
+                       "latency_note": "request latency = arrival to result on the host, over the requests completed "
+                                       "in the window (rank 0); unfinished ages = window end minus arrival of the "
+                                       "requests still queued or running",
                        "l2": "resident scene state of the admitted requests >> 126 MB L2"},
             "roofline": None, "cpu_baseline": cpu,
             "e2e": {"value": work / wall_s, "unit": "96^3-equivalent substeps/s",

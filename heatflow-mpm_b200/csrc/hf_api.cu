@@ -43,6 +43,7 @@ struct DeviceInfo {
     // occupancy of each resident variant [heat][tiles per group][tma][groups] (-1: not queried yet; the query also
     // raises the kernel's dynamic shared-memory limit)
     int res_occ[2][4][2][5];
+    int pipe_occ[4][5];   // the pipelined pressure variant [tiles per group][groups] (-1: not queried yet)
 };
 
 constexpr int kResGroupsMax[4] = {0, 4, 3, 2};   // 256-thread groups per block of the resident variant, by MAXC
@@ -77,6 +78,7 @@ int device_info(DeviceInfo** out) {
         d.smem_optin = (size_t)optin;
         if (!d.coop) return fail(HF_ERR_DEVICE, "device does not support cooperative launches");
         std::memset(d.res_occ, 0xff, sizeof d.res_occ);
+        std::memset(d.pipe_occ, 0xff, sizeof d.pipe_occ);
         d.ready = true;
     }
     *out = &d;
@@ -233,13 +235,15 @@ int launch_resident(const hf_plan* p, DeviceInfo* d, bool heat, double dt, int s
     const bool tma = !(p->options & HF_PLAN_NO_TMA) &&
                      (heat ? (sc.n % 16 == 0 && sc.hkzc && sc.hkx && sc.hky && sc.cell_flags) : (sc.n % 4 == 0));
     const int want = (int)((p->options >> HF_PLAN_RES_TILES_SHIFT) & 3u);   // 0: the first that fits
+    // the pipelined pressure solve (one grid barrier per iteration) when the plan asks for it and the stencil is staged
+    const bool pipe = !heat && tma && (p->options & HF_PLAN_PIPELINED_CG);
     for (int m = want ? want : 1; m <= 3; ++m) {
         const int groups = (tpb + m - 1) / m;
         if (groups > kResGroupsMax[m]) continue;
-        const void* fn = hf::pcg_resident_kernel(heat, m, tma);
-        const size_t smem = hf::pcg_resident_smem(groups, m, tma, heat);
+        const void* fn = pipe ? hf::pcg_pipe_kernel(m) : hf::pcg_resident_kernel(heat, m, tma);
+        const size_t smem = pipe ? hf::pcg_pipe_smem(groups, m) : hf::pcg_resident_smem(groups, m, tma, heat);
         if (smem > d->smem_optin) continue;
-        int& occ = d->res_occ[heat][m][tma][groups];
+        int& occ = pipe ? d->pipe_occ[m][groups] : d->res_occ[heat][m][tma][groups];
         if (occ < 0) {
             if (smem > 48 * 1024)
                 HF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
@@ -475,7 +479,7 @@ int hf_temperature_stage(const hf_plan* p, double dt, void* stream) {
     const hf_scene* scenes = static_cast<const hf_scene*>(p->scenes_dev);
     const hf::WorkItem* work = static_cast<const hf::WorkItem*>(p->work_dev);
     hf::k_prestage<<<p->num_chunks, hf::kThreads, 0, S(stream)>>>(scenes, work, dt);
-    hf::k_advect_T<<<p->num_chunks, hf::kThreads, 0, S(stream)>>>(scenes, work, dt);
+    hf::k_advect_T<<<p->num_chunks * hf::kStageSplit, hf::kThreads, 0, S(stream)>>>(scenes, work, dt);
     HF_CUDA(cudaGetLastError(), "launch (temperature stage)");
     return HF_OK;
 }
@@ -503,7 +507,7 @@ int hf_face_stage(const hf_plan* p, double dt, void* stream) {
     int rc = check_plan(p);
     if (rc) return rc;
     if (!p->num_chunks) return HF_OK;
-    hf::k_face_stage<<<p->num_chunks, hf::kThreads, 0, S(stream)>>>(static_cast<const hf_scene*>(p->scenes_dev),
+    hf::k_face_stage<<<p->num_chunks * hf::kStageSplit, hf::kThreads, 0, S(stream)>>>(static_cast<const hf_scene*>(p->scenes_dev),
                                                                    static_cast<const hf::WorkItem*>(p->work_dev), dt);
     HF_CUDA(cudaGetLastError(), "launch (face stage)");
     return HF_OK;
@@ -570,6 +574,22 @@ int hf_speed_max(const hf_plan* p, int s, float* out_dev, void* stream) {
     hf::k_speed_max<<<592, 256, 0, S(stream)>>>(static_cast<const hf_scene*>(p->scenes_dev), s,
                                                reinterpret_cast<unsigned*>(out_dev));
     HF_CUDA(cudaGetLastError(), "launch (speed max)");
+    return HF_OK;
+}
+
+int hf_set_wait_limit(unsigned long long limit_ns, int absent_block) {
+    if (limit_ns == 0 || limit_ns > 60000000000ull || absent_block < -1)
+        return fail(HF_ERR_ARG, "hf_set_wait_limit: limit must be 1 ns .. 60 s, absent_block >= -1");
+    int rc = hf::set_wait_limit(limit_ns, absent_block);
+    if (rc) return fail(rc, "hf_set_wait_limit: cudaMemcpyToSymbol failed");
+    return HF_OK;
+}
+
+int hf_k_divide_by(int count, const float* x, float y, float* out, void* stream) {
+    if (count < 0 || (count > 0 && (!x || !out)) || !(y != 0.0f)) return fail(HF_ERR_ARG, "hf_k_divide_by: bad arguments");
+    if (count == 0) return HF_OK;
+    hf::k_divide_by<<<592, 256, 0, S(stream)>>>(count, x, y, out);
+    HF_CUDA(cudaGetLastError(), "launch (divide_by)");
     return HF_OK;
 }
 

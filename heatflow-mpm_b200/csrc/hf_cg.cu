@@ -37,6 +37,12 @@
 namespace hf {
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;   // 2 s
+// Limit of every bounded wait of the CG kernels (grid and lane barriers, TMA copies), and the block that does not
+// arrive at the first grid barrier of each persistent CG launch (-1: none).  The defaults are what every solve uses;
+// hf_set_wait_limit changes both, so that a test can make a barrier's wait run out on purpose and check that the
+// kernel reports HF_SCENE_BARRIER_TIMEOUT and returns with the context usable.
+__constant__ unsigned long long c_wait_limit_ns = kBarrierTimeoutNs;
+__constant__ int c_absent_block = -1;
 // Components one group_sum / scene_sums call reduces at most: 3 inner products per tile x 3 tiles of a 256-thread
 // group (the resident variants' set-up).  Every CG kernel's `red` holds kRedComps x 32 doubles (one per warp).
 constexpr int kRedComps = 9;
@@ -54,12 +60,13 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& epoch, int
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned target = epoch * nblocks;
-        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
-        const unsigned long long t0 = global_timer_ns();
+        if (!(epoch == 1 && (int)blockIdx.x == c_absent_block))
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+        const unsigned long long t0 = global_timer_ns(), limit = c_wait_limit_ns;
         unsigned spins = 0;
         while (ld_acquire_u32(bar) < target) {
             if (*(volatile int*)err) break;
-            if ((++spins & 255u) == 0 && global_timer_ns() - t0 > kBarrierTimeoutNs) {
+            if ((++spins & 255u) == 0 && global_timer_ns() - t0 > limit) {
                 atomicExch(err, 1);
                 break;
             }
@@ -119,6 +126,42 @@ __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b
     }
 }
 
+// scene_sums for components comp0 .. comp0 + K - 1 with each component on its own 256 threads (blockDim >= 256 K): the
+// threads 256 q .. 256 q + 255 run exactly the first 256 threads' part of scene_sums for component q, so the sums are
+// bit-identical to scene_sums', with a quarter of the loads and registers per thread.
+template <int K, int STRIDE = 3>
+__device__ __forceinline__ void scene_sums_wide(const double* __restrict__ buf, int b, int e, int comp0, double (&tot)[K],
+                                                double* red) {
+    static_assert(K <= kRedComps, "red holds kRedComps components");
+    const int q = threadIdx.x >> 8, lt = threadIdx.x & 255;
+    double acc = 0.0;
+    if (q < K) {
+        const int cq = comp0 + q;
+        int c = b + lt;
+        for (; c + 3 * kThreads < e; c += 4 * kThreads) {
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = buf[STRIDE * (c + u * kThreads) + cq];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc += v[u];
+        }
+        for (; c < e; c += kThreads) acc += buf[STRIDE * c + cq];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    }
+    const int lane = threadIdx.x & 31, wq = lt >> 5;
+    __syncthreads();
+    if (q < K && lane == 0) red[q * 32 + wq] = acc;
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) s += red[c * 32 + w];
+        tot[c] = s;
+    }
+}
+
 // Per-256-thread-group sum (each group reduces its own 8 warps in index order): the tile partial tree.
 template <int K>
 __device__ __forceinline__ void group_sum(double (&v)[K], double* red) {
@@ -142,6 +185,45 @@ __device__ __forceinline__ void group_sum(double (&v)[K], double* red) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) s += red[c * 32 + g0 + q];
         v[c] = s;
+    }
+}
+
+// group_sum in two steps, so that a thread holds the partials of one tile at a time: stash_warp reduces K values over the
+// warp (the same butterfly) and lane 0 parks them in red[(c0 + c) * 32 + warp]; after every tile's stash,
+// publish_group (thread lt == 0 of each 256-thread group) adds the group's 8 warps in order -- group_sum's tree, the
+// same bits -- and writes the tile partials to buf[3 * tile + c] (3 components per tile).  red must not be read by
+// another phase in between (the caller's barriers see to that).
+template <int K>
+__device__ __forceinline__ void stash_warp(double (&v)[K], double* red, int c0) {
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) red[(c0 + c) * 32 + (threadIdx.x >> 5)] = v[c];
+    }
+}
+
+template <int MAXC>
+__device__ __forceinline__ void publish_group(const double* red, double* __restrict__ buf, int first_tile, int groups,
+                                              int c_end) {
+    __syncthreads();
+    if ((threadIdx.x & 255) == 0) {
+        const int g0 = (threadIdx.x >> 5);   // first warp of this group
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            const int c = first_tile + groups * q;
+            if (c >= c_end) continue;
+#pragma unroll
+            for (int comp = 0; comp < 3; ++comp) {
+                double s = 0.0;
+#pragma unroll
+                for (int w = 0; w < 8; ++w) s += red[(3 * q + comp) * 32 + g0 + w];
+                buf[3 * c + comp] = s;
+            }
+        }
     }
 }
 
@@ -473,7 +555,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phas
             : "r"(smem_addr(bar)), "r"(phase)
             : "memory");
         if (ok) return true;
-        if ((spins & 63u) == 63u && global_timer_ns() - t0 > kBarrierTimeoutNs) return false;
+        if ((spins & 63u) == 63u && global_timer_ns() - t0 > c_wait_limit_ns) return false;
     }
 }
 
@@ -1613,6 +1695,324 @@ finish:
     if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, HEAT, *(volatile int*)ws.err != 0, par);
 }
 
+// ====================================================================== resident pressure CG, one barrier per iteration
+// Pipelined Jacobi-PCG (Ghysels & Vanroose, "Hiding global synchronization latency in the preconditioned Conjugate
+// Gradient algorithm", Parallel Computing 40 (2014), Alg. 4) for the pressure system of one scene with n % 4 == 0.
+// In exact arithmetic it computes the iterates of the classic method above; its recurrences
+//     z = n + beta z,  s = w + beta s,  p = u + beta p,  x += alpha p,  r -= alpha s,  w -= alpha z
+// (u = D r, m = D w, n = A m, w = A u) need a scene sum only of gamma = r.u, delta = w.u and r.r, which are formed in the
+// same place as m, so the halo of m and the three partials are published before ONE grid barrier per iteration
+// (the classic method needs two: after p.Ap and after r.r / r.z).  alpha = gamma / (delta - beta gamma / alpha_old),
+// beta = gamma / gamma_old, in fp64 from the fixed-tree sums and rounded once; u and m are formed from r and w with the
+// diagonal (not by their own recurrences).  The convergence test is the classic one on the recursively updated
+// residual: r.r <= atol^2 with atol = max(tol ||b||, tol, 1e-18), tested before every update, so a converged solve
+// reports the same iteration count.  Rounding differs from the classic method (the vectors follow other
+// recurrences): results agree to ~1e-6 relative, not bit for bit.
+//
+// State: r, w, z, s of a thread's cells in registers; x, p and D of every tile cell in shared memory next to the
+// tile's boxes (the m box with a one-cell halo, restaged by TMA every iteration, and the face fractions, staged once).
+// m is double-buffered in global memory (cg_p[0], cg_p[1]): m_k is written during iteration k-1 and read during k.
+constexpr int kPipeFaces = kBZ;                                 // slot offset of the face-fraction boxes
+constexpr int kPipeCells = kBZ + kBX + kBY + kBW;               // slot offset of x, p, D (1024 floats each)
+constexpr int kPipeSlotFloats = kPipeCells + 3 * 1024;          // 9056 floats = 36,224 bytes (a multiple of 128)
+
+// grid.py:94-115 k_laplacian of one tile cell from a staged box (centre offset o) and the tile's face boxes
+__device__ __forceinline__ float lap_box(const float* __restrict__ B, const float* __restrict__ axb,
+                                         const float* __restrict__ ayb, const float* __restrict__ azb, const Cell& cl,
+                                         int n, int bi, int bj, int bk, int o, float hh) {
+    const float pc = B[o];
+    float acc = 0.0f;
+    if (cl.i > 0) acc = __fadd_rn(acc, __fmul_rn(axb[bi * 256 + bj * 32 + bk], __fsub_rn(pc, B[o - 400])));
+    if (cl.i < n - 1) acc = __fadd_rn(acc, __fmul_rn(axb[(bi + 1) * 256 + bj * 32 + bk], __fsub_rn(pc, B[o + 400])));
+    if (cl.j > 0) acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + bj * 32 + bk], __fsub_rn(pc, B[o - 40])));
+    if (cl.j < n - 1) acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + (bj + 1) * 32 + bk], __fsub_rn(pc, B[o + 40])));
+    if (cl.k > 0) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk], __fsub_rn(pc, B[o - 1])));
+    if (cl.k < n - 1) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk + 1], __fsub_rn(pc, B[o + 1])));
+    return __fdiv_rn(acc, hh);
+}
+
+template <int MAXC>
+__global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
+    k_pcg_pipe(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int tile_lo, int tile_hi,
+               double dt_d, Workspace ws, const __grid_constant__ TileMaps maps) {
+    constexpr int CPT = 4 * MAXC;
+    extern __shared__ __align__(128) float sm_raw[];
+    float* sm_slots = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
+    __shared__ double red[kRedComps * 32];
+    __shared__ LocalScene Ls;
+    __shared__ double s_gamma_old, s_alpha_old;
+    __shared__ __align__(8) unsigned long long mbar[4 * 3];
+    const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
+    const int c0 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * blockIdx.x) / gridDim.x);
+    const int c1 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * (blockIdx.x + 1)) / gridDim.x);
+    const int sidx = tiles[c0].scene;
+    const hf_scene& S = scenes[sidx];
+    const int n = S.n, N = n * n * n;
+    const int par = S.state->parity;
+    unsigned* bar = ws.bar + kMaxLanes;
+    unsigned epoch = 0;
+    const float h = (float)S.h, hh = __fmul_rn(h, h);
+    double* bufA = ws.partA;
+    double* bufB = ws.partB;
+    const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
+    float* xg = S.p;
+    float* const mg0 = S.cg_p[0];
+    float* const mg1 = S.cg_p[1];
+    TileItem my[MAXC];
+    bool have[MAXC];
+#pragma unroll
+    for (int q = 0; q < MAXC; ++q) {
+        const int c = c0 + g + groups * q;
+        have[q] = c < c1;
+        my[q] = tiles[have[q] ? c : c0];
+    }
+    auto slot_of = [&](int q) { return sm_slots + (size_t)(g * MAXC + q) * kPipeSlotFloats; };
+    // stage the m (or u) box of every own tile from buffer b; thread lt == 0 of the group issues
+    auto issue_box = [&](int b) {
+        if (lt == 0) {
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                if (!have[q]) continue;
+                unsigned long long* mb = &mbar[g * MAXC + q];
+                mbar_expect_tx(mb, (unsigned)(kBZ * sizeof(float)));
+                tma_load_3d(slot_of(q), b ? &maps.p1 : &maps.p0, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
+            }
+        }
+    };
+    unsigned phase_bit = 0;
+    auto wait_boxes = [&]() {
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], phase_bit) && ok;
+        if (!ok) atomicExch(ws.err, 1);
+        phase_bit ^= 1u;
+    };
+    if (lt == 0) {
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) mbar_init(&mbar[g * MAXC + q], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    float r[CPT], w[CPT], z[CPT], sv[CPT];
+    int k = 0;
+    // ------------------------------------------------------------------------------------------ set-up
+    float mean = 0.0f;
+    {
+        double mm[1];
+        const int comp[1] = {0};
+        scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red);
+        mean = __double2float_rn(mm[0] / ((double)n * n * n));
+    }
+    {
+        // r0 = b - A x0, u0 = D r0 (published for the halo of w0 = A u0); partials b.b, r.r, r.u
+        __syncthreads();   // red is free (the rhs mean above read it)
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            double part[3] = {0.0, 0.0, 0.0};
+            float* cells = slot_of(q) + kPipeCells;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int s = q * 4 + m, e = m * 256 + lt;
+                r[s] = w[s] = z[s] = sv[s] = 0.0f;
+                cells[e] = cells[1024 + e] = cells[2048 + e] = 0.0f;
+                const Cell cl = tile_cell(my[q], n, lt, m);
+                if (!have[q] || !cl.ok) continue;
+                float b, d, rr;
+                setup_cell<false>(S, xg, mean, hh, 0.0f, cl, b, d, rr);
+                const float u = __fmul_rn(d, rr);
+                cells[e] = xg[cl.t];
+                cells[2048 + e] = d;
+                r[s] = rr;
+                mg0[cl.t] = u;
+                part[0] += (double)b * (double)b;
+                part[1] += (double)rr * (double)rr;
+                part[2] += (double)rr * (double)u;
+            }
+            stash_warp<3>(part, red, 3 * q);
+        }
+        publish_group<MAXC>(red, bufB, c0 + g, groups, c1);
+    }
+    // the tiles' face fractions stay in shared memory for the whole solve
+    if (lt == 0) {
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            if (!have[q]) continue;
+            float* slot = slot_of(q);
+            unsigned long long* mb = &mbar[g * MAXC + q];
+            mbar_expect_tx(mb, (unsigned)((kBX + kBY + kBW) * sizeof(float)));
+            tma_load_3d(slot + kPipeFaces, &maps.ax, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + kPipeFaces + kBX, &maps.ayc, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + kPipeFaces + kBX + kBY, &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
+        }
+    }
+    wait_boxes();
+    if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
+    {
+        double tot[3];
+        const int comp[3] = {0, 1, 2};
+        scene_sums<3>(bufB, cb, ce, comp, tot, red);
+        if (threadIdx.x == 0) {
+            init_scalars(Ls, S, false, tot, N);
+            Ls.mean = (double)mean;
+        }
+        __syncthreads();
+    }
+    if (!Ls.live) goto writeback;
+    {
+        // w0 = A u0 from the staged u0 boxes; partials of iteration 0 (r.u, w.u, r.r); m0 = D w0 published
+        issue_box(0);
+        wait_boxes();
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            double part[3] = {0.0, 0.0, 0.0};
+            const float* slot = slot_of(q);
+            const float* cells = slot + kPipeCells;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int s = q * 4 + m, e = m * 256 + lt;
+                const Cell cl = tile_cell(my[q], n, lt, m);
+                if (!have[q] || !cl.ok) continue;
+                const int bj = lt >> 5, bk = lt & 31, o = (m + 1) * 400 + (bj + 1) * 40 + (bk + 4);
+                const float d = cells[2048 + e];
+                w[s] = lap_box(slot, slot + kPipeFaces, slot + kPipeFaces + kBX, slot + kPipeFaces + kBX + kBY, cl, n, m,
+                               bj, bk, o, hh);
+                const float u = __fmul_rn(d, r[s]);
+                mg1[cl.t] = __fmul_rn(d, w[s]);
+                part[0] += (double)r[s] * (double)u;
+                part[1] += (double)w[s] * (double)u;
+                part[2] += (double)r[s] * (double)r[s];
+            }
+            stash_warp<3>(part, red, 3 * q);
+        }
+        publish_group<MAXC>(red, bufA, c0 + g, groups, c1);
+    }
+    if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
+    // ------------------------------------------------------------------------------------------ iterations
+    for (k = 0;; ++k) {
+        // m_k lives in buffer (k + 1) & 1: request its boxes first, so that the copy overlaps the scene sums
+        issue_box((k + 1) & 1);
+        {
+            double tot[3];
+            const int comp[3] = {0, 1, 2};
+            if (MAXC < 3 && blockDim.x >= 3 * kThreads)   // each component on its own 256 threads
+                scene_sums_wide<3>((k & 1) ? bufB : bufA, cb, ce, 0, tot, red);
+            else
+                scene_sums<3>((k & 1) ? bufB : bufA, cb, ce, comp, tot, red);
+            if (threadIdx.x == 0) {
+                // tot = (gamma_k, delta_k, r_k.r_k); the classic test on r_k before the update of iteration k + 1
+                const double gamma = tot[0], delta = tot[1], rr = tot[2];
+                Ls.iters = k;
+                Ls.rr = rr;
+                Ls.rz = gamma;
+                const bool above = rr > Ls.atol_sq;
+                if (!isfinite(rr)) Ls.status |= HF_SCENE_NONFINITE;
+                const bool live = above && isfinite(rr) && k < Ls.maxit;
+                if (!live && above && isfinite(rr)) Ls.status |= HF_SCENE_PRESSURE_MAXITER;
+                Ls.live = live;
+                if (live) {
+                    double alpha, beta;
+                    if (k == 0) {
+                        beta = 0.0;
+                        alpha = gamma / delta;
+                    } else {
+                        beta = gamma / s_gamma_old;
+                        alpha = gamma / (delta - beta * gamma / s_alpha_old);
+                    }
+                    s_gamma_old = gamma;
+                    s_alpha_old = alpha;
+                    Ls.alpha = __double2float_rn(alpha);
+                    Ls.beta = __double2float_rn(beta);
+                    Ls.pAp = delta;
+                }
+            }
+            __syncthreads();
+        }
+        wait_boxes();
+        if (!Ls.live) break;
+        const float alpha = Ls.alpha, beta = Ls.beta;
+        float* mnext = (k & 1) ? mg1 : mg0;   // m_{k+1}
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            double part[3] = {0.0, 0.0, 0.0};
+            const float* slot = slot_of(q);
+            float* X = slot_of(q) + kPipeCells;
+            float* P = X + 1024;
+            const float* Dg = X + 2048;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int s = q * 4 + m, e = m * 256 + lt;
+                const Cell cl = tile_cell(my[q], n, lt, m);
+                if (!have[q] || !cl.ok) continue;
+                const int bj = lt >> 5, bk = lt & 31, o = (m + 1) * 400 + (bj + 1) * 40 + (bk + 4);
+                const float nv = lap_box(slot, slot + kPipeFaces, slot + kPipeFaces + kBX, slot + kPipeFaces + kBX + kBY,
+                                         cl, n, m, bj, bk, o, hh);
+                const float d = Dg[e];
+                const float u = __fmul_rn(d, r[s]);
+                z[s] = __fadd_rn(nv, __fmul_rn(beta, z[s]));
+                sv[s] = __fadd_rn(w[s], __fmul_rn(beta, sv[s]));
+                const float pk = __fadd_rn(u, __fmul_rn(beta, P[e]));
+                P[e] = pk;
+                X[e] = __fadd_rn(X[e], __fmul_rn(alpha, pk));
+                r[s] = __fsub_rn(r[s], __fmul_rn(alpha, sv[s]));
+                w[s] = __fsub_rn(w[s], __fmul_rn(alpha, z[s]));
+                const float un = __fmul_rn(d, r[s]);
+                mnext[cl.t] = __fmul_rn(d, w[s]);
+                part[0] += (double)r[s] * (double)un;
+                part[1] += (double)w[s] * (double)un;
+                part[2] += (double)r[s] * (double)r[s];
+            }
+            stash_warp<3>(part, red, 3 * q);
+        }
+        publish_group<MAXC>(red, (k & 1) ? bufA : bufB, c0 + g, groups, c1);   // partials of iteration k + 1
+        if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
+    }
+writeback:
+    // -------------------------------------------------- write x back, then project the faces
+#pragma unroll
+    for (int q = 0; q < MAXC; ++q) {
+        const float* X = slot_of(q) + kPipeCells;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const Cell cl = tile_cell(my[q], n, lt, m);
+            if (have[q] && cl.ok) xg[cl.t] = X[m * 256 + lt];
+        }
+    }
+    if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
+    {
+        const float dtr = (float)(dt_d / S.rho);
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            const float* X = slot_of(q) + kPipeCells;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const Cell cl = tile_cell(my[q], n, lt, m);
+                if (have[q] && cl.ok)
+                    project_cell(S, S.u[par ^ 1], S.v[par ^ 1], S.w[par ^ 1], S.p, X[m * 256 + lt], dtr, h, cl);
+            }
+        }
+    }
+finish:
+    if (*(volatile int*)ws.err) {
+        // leave no copy in flight: the last requested boxes are waited for again (bounded) before the block exits
+        // (every request is waited for before the next barrier, so only a wait that gave up can leave one)
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) mbar_wait(&mbar[g * MAXC + q], phase_bit ^ 1u);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, false, *(volatile int*)ws.err != 0, par);
+}
+
+const void* pcg_pipe_kernel(int maxc) {
+    if (maxc == 1) return (const void*)k_pcg_pipe<1>;
+    if (maxc == 2) return (const void*)k_pcg_pipe<2>;
+    return (const void*)k_pcg_pipe<3>;
+}
+
+size_t pcg_pipe_smem(int groups, int maxc) { return (size_t)groups * maxc * kPipeSlotFloats * sizeof(float) + 128; }
+
 const void* pcg_kernel(bool heat, bool tma) {
     return heat ? (const void*)k_pcg<true, false> : tma ? (const void*)k_pcg<false, true> : (const void*)k_pcg<false, false>;
 }
@@ -1638,6 +2038,12 @@ const void* pcg_resident_kernel(bool heat, int maxc, bool tma) {
     if (maxc == 1) return (const void*)k_pcg_res<false, 1, false>;
     if (maxc == 2) return (const void*)k_pcg_res<false, 2, false>;
     return (const void*)k_pcg_res<false, 3, false>;
+}
+
+int set_wait_limit(unsigned long long limit_ns, int absent_block) {
+    if (cudaMemcpyToSymbol(c_wait_limit_ns, &limit_ns, sizeof limit_ns) != cudaSuccess) return HF_ERR_CUDA;
+    if (cudaMemcpyToSymbol(c_absent_block, &absent_block, sizeof absent_block) != cudaSuccess) return HF_ERR_CUDA;
+    return HF_OK;
 }
 
 size_t pcg_resident_smem(int groups, int maxc, bool tma, bool heat) {

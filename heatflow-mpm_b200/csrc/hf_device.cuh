@@ -16,6 +16,11 @@ namespace hf {
 constexpr int kChunk = 1024;      // cells per work item
 constexpr int kThreads = 256;     // threads per block of every chunked kernel
 constexpr int kCellsPerThread = kChunk / kThreads;
+// Blocks per chunk of the gather-bound stages (advection of T, the face stage): one cell per thread, so that a
+// 96^3 scene's 864 chunks make 3456 blocks -- several waves of the 4 resident blocks per SM instead of 1.5, whose
+// second, part-filled wave left most SMs idle.
+constexpr int kStageSplit = 4;
+static_assert(kCellsPerThread % kStageSplit == 0, "a chunk splits into whole cells per thread");
 constexpr double kFxScale = 1099511627776.0;   // 2^40: particle fixed-point scale
 constexpr double kFxInv = 1.0 / 1099511627776.0;
 constexpr int kMaxScenes = 1024;
@@ -38,14 +43,38 @@ __device__ __forceinline__ float maxf_(float a, float b) { return a > b ? a : b;
 // Warp's clamp(x, lo, hi) = min(max(lo, x), hi)
 __device__ __forceinline__ float clampf_(float x, float lo, float hi) { return minf_(maxf_(lo, x), hi); }
 
+// ---------------------------------------------------------------------------- division by a divisor known in advance
+// Correctly rounded x / y when y is fixed for a whole kernel (the cell size h, or h^2), after Brisebarre, Muller &
+// Raina, "Accelerating correctly rounded floating-point division when the divisor is known in advance", IEEE Trans.
+// Computers 53(8), 2004: with zh = RN(1/y) and zl = RN((1 - y zh) / y) (1 - y zh is exact with one FMA), the quotient
+// q = RN(x zh + RN(x zl)) is within one ulp of x / y; one correction step in the manner of Markstein (IBM J. Res. Dev.
+// 34(1), 1990), r = x - q y (exact with one FMA) and RN(q + r zh), rounds it correctly.  Zero, tiny, huge and
+// non-finite x take the ordinary IEEE division, so the result equals __fdiv_rn(x, y) bit for bit for every x (checked
+// against the IEEE division over dense sweeps of x for the cell sizes in use).
+struct DivBy {
+    float y, zh, zl;
+};
+
+__device__ __forceinline__ DivBy div_by(float y) {
+    const float zh = __fdiv_rn(1.0f, y);
+    return DivBy{y, zh, __fdiv_rn(__fmaf_rn(-y, zh, 1.0f), y)};
+}
+
+__device__ __forceinline__ float div_rn(float x, const DivBy& d) {
+    const float ax = fabsf(x);
+    if (!(ax >= 0x1p-96f && ax <= 0x1p96f)) return __fdiv_rn(x, d.y);
+    const float q = __fmaf_rn(x, d.zh, __fmul_rn(x, d.zl));
+    return __fmaf_rn(__fmaf_rn(-q, d.y, x), d.zh, q);
+}
+
 // A sample point in grid units: each coordinate divided by h once (fields.py:14-15 divides before the offset), shared
 // by every lattice sampled at that point.
 struct GridPos {
     float x, y, z;
 };
 
-__device__ __forceinline__ GridPos grid_pos(float px, float py, float pz, float h) {
-    return GridPos{__fdiv_rn(px, h), __fdiv_rn(py, h), __fdiv_rn(pz, h)};
+__device__ __forceinline__ GridPos grid_pos(float px, float py, float pz, const DivBy& h) {
+    return GridPos{div_rn(px, h), div_rn(py, h), div_rn(pz, h)};
 }
 
 // fields.py:5-36 -- trilinear sample of an (nx,ny,nz) lattice with nodes at (i + off) h, indices clamped.
@@ -75,23 +104,58 @@ __device__ __forceinline__ float sample_at(const float* __restrict__ a, GridPos 
 }
 
 __device__ __forceinline__ float sample(const float* __restrict__ a, float px, float py, float pz, float ox, float oy,
-                                        float oz, float h, int nx, int ny, int nz) {
+                                        float oz, const DivBy& h, int nx, int ny, int nz) {
     return sample_at(a, grid_pos(px, py, pz, h), ox, oy, oz, nx, ny, nz);
 }
 
-// fields.py:68-72 (the three lattices at one point: one division per coordinate)
+// One axis of a trilinear sample: the lower node index and the weights of the two nodes, for the lattice offset 0
+// (face lattice along this axis: nodes 0..n) or 0.5 (cell lattice: nodes 0..n-1).  fields.py:14-15, 29-35.
+struct Axis {
+    int i0, i1;
+    float w0, f;
+};
+
+__device__ __forceinline__ Axis axis_at(float q, float off, int nmax) {
+    const float g = __fsub_rn(q, off);
+    const int i = (int)floorf(g);
+    const float f = __fsub_rn(g, (float)i);
+    return Axis{clampi(i, 0, nmax), clampi(i + 1, 0, nmax), __fsub_rn(1.0f, f), f};
+}
+
+// sample_at's eight terms from precomputed axes (the same operations in the same order, so the same bits)
+__device__ __forceinline__ float sample_axes(const float* __restrict__ a, const Axis& X, const Axis& Y, const Axis& Z,
+                                             int sx, int sy) {
+    float s = 0.0f;
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.w0), Z.w0), __ldg(a + X.i0 * sx + Y.i0 * sy + Z.i0)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.w0), Z.f), __ldg(a + X.i0 * sx + Y.i0 * sy + Z.i1)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.f), Z.w0), __ldg(a + X.i0 * sx + Y.i1 * sy + Z.i0)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.f), Z.f), __ldg(a + X.i0 * sx + Y.i1 * sy + Z.i1)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.w0), Z.w0), __ldg(a + X.i1 * sx + Y.i0 * sy + Z.i0)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.w0), Z.f), __ldg(a + X.i1 * sx + Y.i0 * sy + Z.i1)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.f), Z.w0), __ldg(a + X.i1 * sx + Y.i1 * sy + Z.i0)));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.f), Z.f), __ldg(a + X.i1 * sx + Y.i1 * sy + Z.i1)));
+    return s;
+}
+
+// fields.py:68-72 (the three lattices at one point: one division per coordinate).  Along each axis the face lattice
+// (offset 0, nodes 0..n) and the two cell lattices (offset 0.5, nodes 0..n-1) share their node indices and weights,
+// so each axis is resolved twice instead of three times.
 __device__ __forceinline__ void sample_velocity(const float* __restrict__ u, const float* __restrict__ v,
-                                                const float* __restrict__ w, float px, float py, float pz, float h, int n,
-                                                float* o) {
+                                                const float* __restrict__ w, float px, float py, float pz,
+                                                const DivBy& h, int n, float* o) {
     const GridPos q = grid_pos(px, py, pz, h);
-    o[0] = sample_at(u, q, 0.0f, 0.5f, 0.5f, n + 1, n, n);
-    o[1] = sample_at(v, q, 0.5f, 0.0f, 0.5f, n, n + 1, n);
-    o[2] = sample_at(w, q, 0.5f, 0.5f, 0.0f, n, n, n + 1);
+    const Axis x0 = axis_at(q.x, 0.0f, n), x5 = axis_at(q.x, 0.5f, n - 1);
+    const Axis y0 = axis_at(q.y, 0.0f, n), y5 = axis_at(q.y, 0.5f, n - 1);
+    const Axis z0 = axis_at(q.z, 0.0f, n), z5 = axis_at(q.z, 0.5f, n - 1);
+    o[0] = sample_axes(u, x0, y5, z5, n * n, n);               // u: (n+1, n, n)
+    o[1] = sample_axes(v, x5, y0, z5, (n + 1) * n, n);         // v: (n, n+1, n)
+    o[2] = sample_axes(w, x5, y5, z0, n * (n + 1), n + 1);     // w: (n, n, n+1)
 }
 
 // fields.py:111-116: departure point x - dt u(x - dt/2 u(x))
 __device__ __forceinline__ void backtrace(const float* __restrict__ u, const float* __restrict__ v,
-                                          const float* __restrict__ w, const float* x, float h, int n, float dt, float* o) {
+                                          const float* __restrict__ w, const float* x, const DivBy& h, int n, float dt,
+                                          float* o) {
     float vel[3];
     sample_velocity(u, v, w, x[0], x[1], x[2], h, n, vel);
     const float hdt = __fmul_rn(0.5f, dt);

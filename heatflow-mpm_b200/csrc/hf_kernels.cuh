@@ -58,6 +58,7 @@ __global__ void k_speed_max(const hf_scene* __restrict__ scenes, int s, unsigned
 __global__ void k_laplacian_plain(int n, float h, float alpha, float beta, const float* __restrict__ p,
                                   const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ az,
                                   const float* __restrict__ y, float* __restrict__ out);
+__global__ void k_divide_by(int count, const float* __restrict__ x, float y, float* __restrict__ out);
 __global__ void k_heat_matvec_plain(int n, float h, float dt, float alpha, float beta, const float* __restrict__ x,
                                     const float* __restrict__ kap, const uint8_t* __restrict__ fl,
                                     const float* __restrict__ y, float* __restrict__ out);
@@ -73,6 +74,13 @@ size_t pcg_stream_smem(bool tma);
 // scene's tiles; the TileMaps is used when tma; dynamic shared memory pcg_resident_smem(...)
 const void* pcg_resident_kernel(bool heat, int maxc, bool tma);
 size_t pcg_resident_smem(int groups, int maxc, bool tma, bool heat);
+// pipelined register-resident pressure solve of one scene with n % 4 == 0 (one grid barrier per CG iteration), the
+// same arguments and thread layout as the TMA resident variant; dynamic shared memory pcg_pipe_smem(groups, maxc)
+const void* pcg_pipe_kernel(int maxc);
+size_t pcg_pipe_smem(int groups, int maxc);
+// limit of the CG kernels' bounded waits on the current device and the block kept from the first grid barrier
+// (-1: none); synchronous (constant memory)
+int set_wait_limit(unsigned long long limit_ns, int absent_block);
 // device addresses of the per-scene chunk and tile offset tables inside a plan's workspace
 void plan_offset_tables(const hf_plan* p, int** chunk_begin, int** tile_begin);
 // record `msg` as the text of hf_last_error() and return `code`

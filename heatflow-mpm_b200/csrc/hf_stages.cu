@@ -323,9 +323,9 @@ __global__ void __launch_bounds__(kThreads) k_prestage(const hf_scene* __restric
 
 // solver.py:78 k_advect (heat.py:31-41) into T[parity^1], fused with k_heat_rhs (heat.py:108-118) which only needs
 // the advected value of the same cell.
-__global__ void __launch_bounds__(kThreads) k_advect_T(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+__global__ void __launch_bounds__(kThreads, 4) k_advect_T(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
                                                       double dt_d) {
-    const WorkItem wi = work[blockIdx.x];
+    const WorkItem wi = work[blockIdx.x / kStageSplit];
     const hf_scene& S = scenes[wi.scene];
     const int n = S.n, N = n * n * n;
     const int par = S.state->parity;
@@ -335,7 +335,9 @@ __global__ void __launch_bounds__(kThreads) k_advect_T(const hf_scene* __restric
     const float* Tw = S.Tw;
     const uint8_t* fl = S.cell_flags;
     const float c_dt = __fdiv_rn(dt, __fmul_rn(h, h));
-    for (int m = 0; m < kCellsPerThread; ++m) {
+    const DivBy hd = div_by(h);
+    const int m0 = (int)(blockIdx.x % kStageSplit) * (kCellsPerThread / kStageSplit);
+    for (int m = m0; m < m0 + kCellsPerThread / kStageSplit; ++m) {
         const int t = wi.first + threadIdx.x + m * kThreads;
         if (t >= N) break;
         int i, j, k;
@@ -347,8 +349,8 @@ __global__ void __launch_bounds__(kThreads) k_advect_T(const hf_scene* __restric
             float x[3] = {__fmul_rn(__fadd_rn((float)i, 0.5f), h), __fmul_rn(__fadd_rn((float)j, 0.5f), h),
                           __fmul_rn(__fadd_rn((float)k, 0.5f), h)};
             float y[3];
-            backtrace(u, v, w, x, h, n, dt, y);
-            out = sample(Tw, y[0], y[1], y[2], 0.5f, 0.5f, 0.5f, h, n, n, n);
+            backtrace(u, v, w, x, hd, n, dt, y);
+            out = sample(Tw, y[0], y[1], y[2], 0.5f, 0.5f, 0.5f, hd, n, n, n);
         }
         T2[t] = out;
         // heat rhs: tfix on fixed cells, else T2 + dt/h^2 * sum over fixed neighbours of kappa_f * tfix
@@ -395,7 +397,7 @@ __global__ void __launch_bounds__(kThreads) k_particle_update(const hf_scene* __
     const float t_sol = (float)S.t_sol, t_liq = (float)S.t_liq, y_solid = (float)S.y_solid;
     const float mu_s = (float)S.mu_s, mu_l = (float)S.mu_l, t_max = (float)S.t_max;
     const float px = S.pos[3 * t], py = S.pos[3 * t + 1], pz = S.pos[3 * t + 2];
-    const GridPos q = grid_pos(px, py, pz, h);
+    const GridPos q = grid_pos(px, py, pz, div_by(h));
     const float dT = __fsub_rn(sample_at(S.T[par ^ 1], q, 0.5f, 0.5f, 0.5f, n, n, n),
                                sample_at(S.Tw, q, 0.5f, 0.5f, 0.5f, n, n, n));
     const float tp = clampf_(__fadd_rn(S.ptemp[t], dT), 0.0f, t_max);
@@ -412,14 +414,15 @@ __global__ void __launch_bounds__(kThreads) k_particle_update(const hf_scene* __
 // values, so applying the three kernels face by face is the same arithmetic as the reference's three passes.
 __device__ __forceinline__ float relax_face(float q, float af, float kf, float mf, float rho, float afmin, float h,
                                             float dt) {
-    const float c = __fdiv_rn(1.0f, __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(rho, maxf_(af, afmin)), h), h), h));
+    // 1 / (...) correctly rounded: __frcp_rn is the IEEE round-to-nearest reciprocal, the same value as __fdiv_rn(1, .)
+    const float c = __frcp_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(rho, maxf_(af, afmin)), h), h), h));
     const float dtc = __fmul_rn(dt, c);
     return __fdiv_rn(__fadd_rn(q, __fmul_rn(dtc, mf)), __fadd_rn(1.0f, __fmul_rn(dtc, kf)));
 }
 
-__global__ void __launch_bounds__(kThreads) k_face_stage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+__global__ void __launch_bounds__(kThreads, 4) k_face_stage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
                                                         double dt_d) {
-    const WorkItem wi = work[blockIdx.x];
+    const WorkItem wi = work[blockIdx.x / kStageSplit];
     const hf_scene& S = scenes[wi.scene];
     const int n = S.n, N = n * n * n;
     const int par = S.state->parity;
@@ -429,8 +432,10 @@ __global__ void __launch_bounds__(kThreads) k_face_stage(const hf_scene* __restr
     const float h = (float)S.h, dt = (float)dt_d, rho = (float)S.rho, afmin = (float)S.alpha_f_min;
     const float g = (float)S.g, t_amb = (float)S.t_amb;
     const bool buoy = (S.flags & HF_FLAG_BUOYANCY) != 0;
-    const float buoy_num = __fmul_rn(dt, g), buoy_den = __fadd_rn(t_amb, 273.15f);
-    for (int m = 0; m < kCellsPerThread; ++m) {
+    const float buoy_num = __fmul_rn(dt, g);
+    const DivBy hd = div_by(h), buoy_den = div_by(__fadd_rn(t_amb, 273.15f));
+    const int m0 = (int)(blockIdx.x % kStageSplit) * (kCellsPerThread / kStageSplit);
+    for (int m = m0; m < m0 + kCellsPerThread / kStageSplit; ++m) {
         const int t = wi.first + threadIdx.x + m * kThreads;
         if (t >= N) break;
         int i, j, k;
@@ -445,8 +450,8 @@ __global__ void __launch_bounds__(kThreads) k_face_stage(const hf_scene* __restr
             float val = 0.0f;
             if (i != 0) {
                 const float x[3] = {__fmul_rn(fi, h), cj, ck};
-                backtrace(u0, v0, w0, x, h, n, dt, y);
-                val = sample(u0, y[0], y[1], y[2], 0.0f, 0.5f, 0.5f, h, n + 1, n, n);
+                backtrace(u0, v0, w0, x, hd, n, dt, y);
+                val = sample(u0, y[0], y[1], y[2], 0.0f, 0.5f, 0.5f, hd, n + 1, n, n);
                 val = relax_face(val, S.ax[f], S.kx[f], S.mx[f], rho, afmin, h, dt);
             }
             u1[f] = val;
@@ -458,8 +463,8 @@ __global__ void __launch_bounds__(kThreads) k_face_stage(const hf_scene* __restr
             float val = 0.0f;
             if (j != 0) {
                 const float x[3] = {ci, __fmul_rn(fj, h), ck};
-                backtrace(u0, v0, w0, x, h, n, dt, y);
-                val = sample(v0, y[0], y[1], y[2], 0.5f, 0.0f, 0.5f, h, n, n + 1, n);
+                backtrace(u0, v0, w0, x, hd, n, dt, y);
+                val = sample(v0, y[0], y[1], y[2], 0.5f, 0.0f, 0.5f, hd, n, n + 1, n);
                 val = relax_face(val, S.ay[f], S.ky[f], S.my[f], rho, afmin, h, dt);
             }
             v1[f] = val;
@@ -471,11 +476,11 @@ __global__ void __launch_bounds__(kThreads) k_face_stage(const hf_scene* __restr
             float val = 0.0f;
             if (k != 0) {
                 const float x[3] = {ci, cj, __fmul_rn(fk, h)};
-                backtrace(u0, v0, w0, x, h, n, dt, y);
-                val = sample(w0, y[0], y[1], y[2], 0.5f, 0.5f, 0.0f, h, n, n, n + 1);
+                backtrace(u0, v0, w0, x, hd, n, dt, y);
+                val = sample(w0, y[0], y[1], y[2], 0.5f, 0.5f, 0.0f, hd, n, n, n + 1);
                 if (buoy) {
                     const float tf = __fmul_rn(0.5f, __fadd_rn(Tn[t - 1], Tn[t]));
-                    val = __fadd_rn(val, __fdiv_rn(__fmul_rn(buoy_num, __fsub_rn(tf, t_amb)), buoy_den));
+                    val = __fadd_rn(val, div_rn(__fmul_rn(buoy_num, __fsub_rn(tf, t_amb)), buoy_den));
                 }
                 val = relax_face(val, S.az[f], S.kz[f], S.mz[f], rho, afmin, h, dt);
             }
@@ -587,6 +592,12 @@ __global__ void k_speed_max(const hf_scene* __restrict__ scenes, int s, unsigned
 }
 
 // ------------------------------------------------------------------------------------- single-kernel parity
+// the constant-divisor division of the sampling stages, elementwise (checked against IEEE division)
+__global__ void k_divide_by(int count, const float* __restrict__ x, float y, float* __restrict__ out) {
+    const DivBy d = div_by(y);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) out[i] = div_rn(x[i], d);
+}
+
 // grid.py:94-115 k_laplacian on plain arrays
 __global__ void k_laplacian_plain(int n, float h, float alpha, float beta, const float* __restrict__ p,
                                   const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ az,

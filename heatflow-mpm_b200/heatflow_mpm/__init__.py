@@ -2,7 +2,7 @@
 from .grid import GridConfig, AirGrid  # noqa: F401
 from .heat import HeatField  # noqa: F401
 from .heater import Heater, BoxHeater  # noqa: F401
-from .mpm import Material, ThermalMPM, FrozenBody  # noqa: F401
+from .mpm import DLPackBody, Material, ThermalMPM, FrozenBody  # noqa: F401
 from .solver import HeatflowMPM, KAPPA_AIR  # noqa: F401
 from .batch import AirScenario, AirBatch, autotune, ensemble, shard_scenarios  # noqa: F401
 from .serve import AirServer, Request, poisson_trace  # noqa: F401

@@ -15,10 +15,12 @@ HF_OK, HF_ERR_ARG, HF_ERR_CUDA, HF_ERR_WORKSPACE, HF_ERR_DEVICE = 0, 1, 2, 3, 4
 HF_FLAG_BUOYANCY, HF_FLAG_SOURCE, HF_FLAG_PARTICLES, HF_FLAG_ACTIVE, HF_FLAG_DEFECT_CORRECTION = 1, 2, 4, 8, 16
 HF_SCENE_CORRECTED = 16
 HF_SCENE_HEAT_MAXITER, HF_SCENE_PRESSURE_MAXITER, HF_SCENE_NONFINITE, HF_SCENE_BARRIER_TIMEOUT = 1, 2, 4, 8
+WAIT_LIMIT_NS = 2_000_000_000   # default limit of the CG kernels' bounded waits (hf_set_wait_limit)
 CHUNK = 1024
 HF_PLAN_STREAMING_CG = 1
 HF_PLAN_NO_TMA = 2
 HF_PLAN_STREAMING_HEAT = 4
+HF_PLAN_PIPELINED_CG = 8
 HF_PLAN_LANES_SHIFT = 8
 HF_PLAN_RES_TILES_SHIFT = 12
 
@@ -107,6 +109,8 @@ def load():
     L.hf_winding_inside.argtypes = [_P, C.c_int, _P, C.c_int, C.c_float, _P, _P, _P]
     L.hf_k_laplacian.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double] + [_P] * 6 + [_P]
     L.hf_k_heat_matvec.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double] + [_P] * 5 + [_P]
+    L.hf_k_divide_by.argtypes = [C.c_int, _P, C.c_float, _P, _P]
+    L.hf_set_wait_limit.argtypes = [C.c_ulonglong, C.c_int]
     if L.hf_abi_version() != 1:
         raise HeatflowError("libheatflow_b200.so ABI version mismatch")
     _lib = L

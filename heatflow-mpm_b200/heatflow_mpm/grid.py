@@ -87,9 +87,22 @@ class AirGrid:
         return int(self._scene.read_state().pressure_iters)
 
     def set_static(self, alpha, k_faces, m_faces):
-        """grid.py:198-200 -- kept for API compatibility; statics are fixed when the scene is built."""
-        self.static = (np.asarray(alpha, np.float32), [np.asarray(a, np.float32) for a in k_faces],
-                       [np.asarray(a, np.float32) for a in m_faces])
+        """grid.py:198-200: replace the static obstacle fields (solid fraction (n,n,n); relaxation weights k and
+        momentum m on the three face lattices) that every substep adds to the particle contributions (grid.py:206-213).
+        The new arrays are copied into the scene's device statics and the obstacle fields, face fractions and
+        conductivity are rebuilt from them at once, so the next substep uses them (a recorded substep graph stays
+        valid: it reads the same buffers)."""
+        n = self.n
+        alpha = np.asarray(alpha, np.float32)
+        ks = [np.asarray(a, np.float32) for a in k_faces]
+        ms = [np.asarray(a, np.float32) for a in m_faces]
+        shapes = [(n + 1, n, n), (n, n + 1, n), (n, n, n + 1)]
+        if alpha.shape != (n, n, n) or [a.shape for a in ks] != shapes or [a.shape for a in ms] != shapes:
+            raise ValueError("set_static: alpha (n,n,n) and three k and m face arrays of the MAC lattices expected")
+        self.static = (alpha, ks, ms)
+        if self._scene is not None:
+            self._scene.set_statics(alpha, ks, ms)
+            self._plan.prepare_statics()
 
     def cell_velocity(self) -> np.ndarray:
         """grid.py:253-255: cell-centred velocity (n^3, 3) float32 on the host."""

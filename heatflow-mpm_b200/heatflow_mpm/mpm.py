@@ -1,7 +1,8 @@
 """Material particles (reference: heatflow_mpm/mpm.py).  ``Material`` is the reference's dataclass.  ``ThermalMPM`` keeps
 NVIDIA Newton's SolverImplicitMPM as the material solver (imported lazily, as the reference does), exchanging particle
 arrays with the air path through DLPack.  ``FrozenBody`` is a stand-in body whose particles keep their positions and
-velocities; it drives the coupled air path when Newton is not installed (synthetic benchmarks, parity tests)."""
+velocities; it drives the coupled air path when Newton is not installed (synthetic benchmarks, parity tests).
+``DLPackBody`` is the exchange itself, for any material solver whose arrays speak DLPack."""
 from __future__ import annotations
 
 from dataclasses import dataclass
@@ -59,7 +60,44 @@ class FrozenBody:
         return self.vel_t.cpu().numpy()
 
 
-class ThermalMPM:
+def dlpack_view(arr) -> torch.Tensor:
+    """A zero-copy torch view of another framework's device array: through the DLPack protocol (``__dlpack__``, which
+    Warp, CuPy, JAX and torch arrays implement) or, for arrays without it, Warp's ``to_dlpack`` capsule."""
+    if hasattr(arr, "__dlpack__"):
+        return torch.from_dlpack(arr)
+    import warp as wp
+    return torch.from_dlpack(wp.to_dlpack(arr))
+
+
+class DLPackBody:
+    """The material side of the air substep (mpm.py:54-68, heat.py:161-174) for a solver that owns its particle arrays:
+    positions and velocities are read, and yield stress and viscosity written, through zero-copy DLPack views of the
+    solver's own device arrays -- no host copies and no extra device buffers.  A subclass names the arrays
+    (``dlpack_arrays``: particle_q (P,3), particle_qd (P,3), yield_stress (P), viscosity (P)) and advances the solver
+    (``step``)."""
+
+    def dlpack_arrays(self):
+        raise NotImplementedError
+
+    def particle_state(self):
+        q, qd, _, _ = self.dlpack_arrays()
+        return dlpack_view(q).view(-1, 3), dlpack_view(qd).view(-1, 3)
+
+    def material_outputs(self):
+        _, _, ys, visc = self.dlpack_arrays()
+        return dlpack_view(ys), dlpack_view(visc)
+
+    def step(self, dt: float):
+        raise NotImplementedError
+
+    def positions(self) -> np.ndarray:
+        return self.particle_state()[0].cpu().numpy()
+
+    def velocities(self) -> np.ndarray:
+        return self.particle_state()[1].cpu().numpy()
+
+
+class ThermalMPM(DLPackBody):
     """mpm.py:25-80: Newton implicit MPM body; its particle state is read, and its yield stress and viscosity written,
     through zero-copy DLPack views."""
 
@@ -94,13 +132,8 @@ class ThermalMPM:
             self.solver = SolverImplicitMPM(self.model, config=cfg)
             self.s0, self.s1 = self.model.state(), self.model.state()
 
-    def particle_state(self):
-        return (torch.from_dlpack(self._wp.to_dlpack(self.s0.particle_q)).view(-1, 3),
-                torch.from_dlpack(self._wp.to_dlpack(self.s0.particle_qd)).view(-1, 3))
-
-    def material_outputs(self):
-        return (torch.from_dlpack(self._wp.to_dlpack(self.model.mpm.yield_stress)),
-                torch.from_dlpack(self._wp.to_dlpack(self.model.mpm.viscosity)))
+    def dlpack_arrays(self):
+        return self.s0.particle_q, self.s0.particle_qd, self.model.mpm.yield_stress, self.model.mpm.viscosity
 
     def step(self, dt: float):
         with self._wp.ScopedDevice(self.dev):

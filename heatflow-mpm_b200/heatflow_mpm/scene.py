@@ -160,6 +160,23 @@ class DeviceScene:
         self.fill_record()
         self.dirty = True
 
+    def set_statics(self, alpha, k_faces, m_faces):
+        """New static obstacle fields (grid.py:198-200), copied into the scene's static buffers.  A scene built without
+        statics gets buffers now (its record changes: the plan is uploaded again before its next launch).  The caller
+        rebuilds the obstacle fields (ScenePlan.prepare_statics)."""
+        dev = self.device
+        up = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
+        if self.st_alpha is None:
+            self.st_alpha, self.st_k, self.st_m = up(alpha), [up(a) for a in k_faces], [up(a) for a in m_faces]
+            if self.spec.n_particles == 0:    # air-only scenes use the statics as their obstacle fields
+                self.alpha_s, self.k, self.m = self.st_alpha, list(self.st_k), list(self.st_m)
+            self.fill_record()
+            self.dirty = True
+            return
+        self.st_alpha.copy_(up(alpha))
+        for dst, a in zip(list(self.st_k) + list(self.st_m), list(k_faces) + list(m_faces)):
+            dst.copy_(up(a))
+
     def apply_fixed_to_T(self):
         T = self.T[self.parity()]
         f = (self.cell_flags & 1).bool()
@@ -277,6 +294,19 @@ class ScenePlan:
         if not 0 <= int(m) <= 3:
             raise ValueError("resident_tiles must be 0..3")
         self.plan.options = (self.plan.options & ~(3 << _lib.HF_PLAN_RES_TILES_SHIFT)) | (int(m) << _lib.HF_PLAN_RES_TILES_SHIFT)
+
+    @property
+    def pipelined_cg(self):
+        """Pressure solve of a single-scene plan (n % 4 == 0) by pipelined Jacobi-PCG: one grid barrier per iteration,
+        the same stopping rule, rounding that differs from the classic method by ~1e-6 relative.  Off by default."""
+        return bool(self.plan.options & _lib.HF_PLAN_PIPELINED_CG)
+
+    @pipelined_cg.setter
+    def pipelined_cg(self, on):
+        if on:
+            self.plan.options |= _lib.HF_PLAN_PIPELINED_CG
+        else:
+            self.plan.options &= ~_lib.HF_PLAN_PIPELINED_CG
 
     def stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)

@@ -28,7 +28,7 @@ def ellipsoid_particles(semi=(0.04, 0.03, 0.05), spacing=2.5e-3, L=0.48, seed=0,
     return (P + np.array([L / 2, L / 2, spacing / 2])).astype(np.float32)
 
 
-def coupled_default(device="cuda:0", body="frozen", seed=0, persistent_blocks=0):
+def coupled_default(device="cuda:0", body="frozen", seed=0, persistent_blocks=0, cg="classic"):
     from .grid import GridConfig
     from .heater import Heater
     from .mpm import Material
@@ -38,7 +38,7 @@ def coupled_default(device="cuda:0", body="frozen", seed=0, persistent_blocks=0)
     heater = Heater(power=400.0, t_cap=120.0, fan=2.0, t_rod=300.0)
     grid = GridConfig(L=0.48, h=0.005, t_amb=25.0)
     return HeatflowMPM(parts, mat=mat, heater=heater, grid=grid, spacing=2.5e-3, t_init=20.0, device=device, body=body,
-                       persistent_blocks=persistent_blocks)
+                       persistent_blocks=persistent_blocks, cg=cg)
 
 
 PRECISION_FOOTPRINT = 5800     # cells covered by the precision-study body

@@ -122,6 +122,11 @@ typedef struct hf_scene {
                                         the scene's tiles fit one block per SM) */
 #define HF_PLAN_NO_TMA 2u            /* resident pressure CG without the TMA-staged stencil */
 #define HF_PLAN_STREAMING_HEAT 4u    /* the heat CG of a single-scene plan in the streaming kernel (pressure unchanged) */
+#define HF_PLAN_PIPELINED_CG 8u      /* single-scene plans with n % 4 == 0: the pressure solve by pipelined Jacobi-PCG
+                                        (Ghysels & Vanroose 2014; one grid barrier per iteration instead of two).  Same
+                                        stopping rule (r.r <= atol^2 on the recursive residual) and, in exact
+                                        arithmetic, the same iterates; the binary32 rounding differs from the classic
+                                        method (agreement ~1e-6 relative), so it is off by default. */
 #define HF_PLAN_MAPS_READY 0x8000u   /* set by hf_plan_upload: the workspace holds the scenes' TMA descriptors (the
                                         streaming pressure CG stages its stencil boxes with TMA when every active scene
                                         has n % 4 == 0) */
@@ -210,6 +215,18 @@ int hf_k_laplacian(int n, double h, double alpha, double beta, const float *p, c
 /* heat.py:94-105 k_heat_matvec */
 int hf_k_heat_matvec(int n, double h, double dt, double alpha, double beta, const float *x, const float *kap,
                      const uint8_t *cell_flags, const float *y, float *out, void *stream);
+/* The division by the cell size that every sampling stage performs (fields.py:14-15 divides each coordinate of a
+   sample point by h): out[i] = x[i] / y, correctly rounded, by the kernels' constant-divisor method (a precomputed
+   reciprocal pair and one correction; see hf_device.cuh).  For checking that method against IEEE division. */
+int hf_k_divide_by(int count, const float *x, float y, float *out, void *stream);
+
+/* Failure detection (no counterpart in the reference, whose solves cannot time out).  Every spin-wait of the persistent
+   CG kernels -- grid and lane barriers, TMA copies -- gives up after limit_ns (default 2 s), sets
+   HF_SCENE_BARRIER_TIMEOUT in the scenes of the launch, and every block returns, leaving the context usable.
+   absent_block >= 0 keeps that block of each CG launch from arriving at its first grid barrier, so that a test can
+   make the wait run out on purpose (-1: normal operation).  Applies to later launches on the current device;
+   synchronous.  Restore (2000000000, -1) after a test. */
+int hf_set_wait_limit(unsigned long long limit_ns, int absent_block);
 
 /* ------------------------------------------------------------------------------------ scene set-up on the device */
 /* Geometry of one scene's heater and optional static sphere.  The host fills it from the heater's parameters: the

@@ -82,9 +82,19 @@ def test_admission_respects_slots_and_hbm_budget(monkeypatch):
     monkeypatch.setattr(serve, "make_scene", lambda sc, dev, **kw: setups.append(kw.get("setup")) or object())
     monkeypatch.setattr(serve, "ScenePlan", FakePlan)
 
+    class Landed:                                          # a result copy that has already landed
+        def query(self):
+            return True
+
+        def synchronize(self):
+            pass
+
     class Server(serve.AirServer):
         def _advance(self):
-            return 0.0
+            pass
+
+        def _copy_back(self, req, slot):
+            return Landed(), {}
 
     big, small = AirScenario(n=96, horizon=3), AirScenario(n=32, horizon=2)
     srv = Server(device="cpu", hbm_budget=big.device_bytes() + 2 * small.device_bytes(), max_slots=3, result_fields=())
@@ -229,3 +239,37 @@ def test_autotune_keeps_results(cuda):
             b.substep(2e-3)
         assert same(b, ref), (pb, gc, ln)
         assert [s.read_state().pressure_iters for s in b.scenes] == [s.read_state().pressure_iters for s in ref.scenes]
+
+
+@pytest.mark.gpu
+def test_served_failure_is_reported_for_that_request_only(cuda):
+    """Three requests served together; after the first batched substep a NaN is written on the host into the middle
+    request's temperature.  The server's status check finds HF_SCENE_NONFINITE, that request leaves the batch as
+    failed (its result carries the status), and the other two finish with results bit-identical to running alone."""
+    import dataclasses
+    from heatflow_mpm import _lib
+    from heatflow_mpm.serve import AirServer, Request
+    scs = [dataclasses.replace(sc, horizon=h) for sc, h in zip(_scenarios()[:3], (5, 6, 4))]
+    srv = AirServer(max_slots=3, keep_results=True, status_every=2)
+    reqs = [Request(sc, 0.0, i) for i, sc in enumerate(scs)]
+    for r in reqs:
+        srv.submit(r)
+    t = 0.0
+    srv.step(t)
+    bad = reqs[1]
+    T = bad.scene.current("T").cpu().numpy()
+    T[3, 4, 5] = np.nan
+    bad.scene.set_current("T", T)
+    while srv.queue or srv.active or srv.retiring:
+        t += 0.01
+        srv.step(t)
+        srv._collect(t, wait=not srv.active)
+    cuda.cuda.synchronize()
+    assert [r.rid for r in srv.failed] == [1] and sorted(r.rid for r in srv.finished) == [0, 2]
+    assert bad.result["failed"] and bad.result["status"] & _lib.HF_SCENE_NONFINITE
+    assert bad.substeps_done < bad.scenario.horizon          # it left the batch before its horizon
+    for r in srv.finished:
+        assert r.substeps_done == r.scenario.horizon
+        _same(r.result, r.result["state"], _alone(r.scenario, r.scenario.horizon))
+    s = srv.summary()
+    assert s["requests_failed"] == 1 and s["requests_done"] == 2

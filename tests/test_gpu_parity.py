@@ -83,8 +83,10 @@ def test_substeps_vs_reference_and_oracle(torch_cuda, name):
             assert np.allclose(sc.pmelt.cpu().numpy(), fx[f"pmelt_{s}"], atol=1e-5)
 
 
-def test_larger_scene_vs_oracle(torch_cuda):
-    """n = 32 with the reference trough heater (fan on), 4 substeps: GPU vs oracle (build arithmetic)."""
+@pytest.mark.parametrize("cg", ["classic", "pipelined"])
+def test_larger_scene_vs_oracle(torch_cuda, cg):
+    """n = 32 with the reference trough heater (fan on), 4 substeps: GPU vs oracle (build arithmetic).  The pipelined
+    pressure solve rounds differently from the classic method the oracle restates: relative L2 <= 1e-5 for it."""
     from heatflow_mpm.scene import DeviceScene, ScenePlan
     spec, T0, uvw = random_scene_inputs(32, seed=21)
     spec.cg_tol = 1e-6
@@ -93,6 +95,8 @@ def test_larger_scene_vs_oracle(torch_cuda):
         sc.set_current(nm, a)
     sc.set_current("T", T0)
     plan = ScenePlan([sc])
+    plan.pipelined_cg = cg == "pipelined"
+    tol = 1e-6 if cg == "classic" else 1e-5
     plan.prepare_statics()
     orc = oracle_from_spec(spec)
     orc.set_state(T=T0, u=uvw[0], v=uvw[1], w=uvw[2])
@@ -101,9 +105,10 @@ def test_larger_scene_vs_oracle(torch_cuda):
         orc.substep(2e-3)
         for nm in ("T", "u", "v", "w"):
             got = sc.current(nm).cpu().numpy()
-            assert rel_l2(got, getattr(orc, nm)) <= 1e-6, (nm, s)
+            assert rel_l2(got, getattr(orc, nm)) <= tol, (nm, s, rel_l2(got, getattr(orc, nm)))
         st, ost = sc.read_state(), orc.stats()
         assert st.status == 0
+        assert st.pressure_rr <= st.pressure_atol ** 2 * (1 + 1e-12)
         assert abs(st.pressure_iters - ost["grid_done"]) <= 2
 
 
@@ -218,20 +223,23 @@ def test_config1_air_only_plume_100_substeps(torch_cuda):
     assert sim.grid.divergence_max() < 1e-3
 
 
-def test_headline_coupled96_vs_oracle(torch_cuda):
+@pytest.mark.parametrize("cg", ["classic", "pipelined"])
+def test_headline_coupled96_vs_oracle(torch_cuda, cg):
     """The benchmark's own configuration -- the default coupled 96^3 scene (h = 5 mm, trough heater 400 W capped at
     120 C, fan 2 m/s, ~16k-particle ellipsoid, frozen body) -- through HeatflowMPM.substep (CUDA-graph replay, the
     TMA-staged resident CG variants, the footprint-box obstacle rebuild): 30 spin-up substeps, then 20 substeps on the
     GPU and on the oracle from the same state.  Every substep: the same CG iteration counts (within 2 for the pressure
     solve, 1 for heat), every solve converged (r.r <= atol^2, status 0); at the end relative L2 <= 1e-6 for T, u, v,
-    w and the particle temperatures."""
+    w and the particle temperatures with the classic pressure solve (the oracle's method), <= 1e-5 with the pipelined
+    one (other rounding)."""
     torch = torch_cuda
     from heatflow_mpm.synthetic import coupled_default
     from oracle import oracle as O
     from helpers import coupled_default_oracle
     import os
     O.set_threads(len(os.sched_getaffinity(0)))
-    sim = coupled_default()
+    tol = 1e-6 if cg == "classic" else 1e-5
+    sim = coupled_default(cg=cg)
     sc = sim.scene
     for _ in range(30):
         sim.substep(2e-3)
@@ -251,5 +259,96 @@ def test_headline_coupled96_vs_oracle(torch_cuda):
         assert st.heat_rr <= st.heat_atol ** 2 * (1 + 1e-12)
     for nm in ("T", "u", "v", "w"):
         got = sc.current(nm).cpu().numpy()
-        assert rel_l2(got, getattr(orc, nm)) <= 1e-6, (nm, rel_l2(got, getattr(orc, nm)))
-    assert rel_l2(sc.ptemp.cpu().numpy(), orc.a["ptemp"][: sim.n]) <= 1e-6
+        assert rel_l2(got, getattr(orc, nm)) <= tol, (nm, rel_l2(got, getattr(orc, nm)))
+    assert rel_l2(sc.ptemp.cpu().numpy(), orc.a["ptemp"][: sim.n]) <= tol
+
+
+def test_divide_by_constant_matches_ieee(torch_cuda):
+    """The sampling stages divide every sample coordinate by the cell size with a precomputed reciprocal pair and one
+    correction step instead of an IEEE division; the result must be the correctly rounded quotient bit for bit.
+    Reference: the binary64 quotient of the two binary32 operands rounded to binary32 (double rounding is harmless for
+    division when the intermediate has >= 2p + 2 bits).  Every binary32 value in [2^-12, 2^9) (both signs) and 16 M
+    random bit patterns over the whole range (zeros, subnormals, infinities and NaNs included), for the cell sizes of
+    the test and benchmark scenes and the buoyancy denominator."""
+    torch = torch_cuda
+    from heatflow_mpm import _lib
+    L = _lib.load()
+    L.hf_k_divide_by.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p]
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    divisors = {np.float32(v) for v in (0.01, 0.015, 0.005, 0.003, 0.02, 298.15)}
+    divisors |= {np.float32(0.48 / n) for n in (32, 48, 64, 96, 128, 160)}
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    rnd = torch.randint(-2 ** 31, 2 ** 31 - 1, (1 << 24,), device="cuda", dtype=torch.int64, generator=gen).to(torch.int32)
+    lo, hi = np.float32(2.0 ** -12).view(np.int32), np.float32(2.0 ** 9).view(np.int32)
+    chunk = 1 << 24
+    for y in sorted(divisors):
+        def check(xbits):
+            x = xbits.view(torch.float32)
+            out = torch.empty_like(x)
+            _lib.check(L.hf_k_divide_by(x.numel(), C.c_void_p(x.data_ptr()), C.c_float(float(y)),
+                                        C.c_void_p(out.data_ptr()), stream))
+            ref = (x.double() / float(y)).float()
+            same = (out.view(torch.int32) == ref.view(torch.int32)) | (torch.isnan(out) & torch.isnan(ref))
+            bad = int((~same).sum())
+            if bad:
+                i = int((~same).nonzero()[0])
+                raise AssertionError(f"y={y!r}: {bad} mismatches, e.g. x={float(x[i])!r}: {float(out[i])!r} "
+                                     f"vs {float(ref[i])!r}")
+        for start in range(int(lo), int(hi), chunk):
+            b = torch.arange(start, min(start + chunk, int(hi)), device="cuda", dtype=torch.int64).to(torch.int32)
+            check(b)
+            check(b | torch.tensor(-2 ** 31, dtype=torch.int32, device="cuda"))   # negative values
+        check(rnd)
+        check(torch.tensor([0, -2 ** 31, 1, 0x7F800000, -8388608, 0x7FC00000], dtype=torch.int32, device="cuda"))
+
+
+def test_sampling_stages_bit_exact_vs_oracle(torch_cuda):
+    """The face stage (semi-Lagrangian advection of u, v, w + buoyancy + relaxation, grid.py:25-79) and the temperature
+    stage's advection (heat.py:21-41 with the blend, fixed cells and source) against the oracle's kernels, bit for bit
+    (compared as integers), on a random air-only scene whose velocities carry back-traces outside the domain."""
+    torch = torch_cuda
+    from heatflow_mpm.scene import DeviceScene, ScenePlan
+    from oracle.oracle import Kernels
+    n, dt = 20, 2e-3
+    spec, T0, uvw = random_scene_inputs(n, seed=9)
+    rng = np.random.default_rng(4)
+    uvw = [rng.uniform(-3.0, 3.0, a.shape).astype(np.float32) for a in uvw]
+    sc = DeviceScene(spec)
+    plan = ScenePlan([sc])
+    plan.prepare_statics()
+    par = sc.parity()
+    for nm, a in zip("uvw", uvw):
+        getattr(sc, nm)[par].copy_(torch.as_tensor(a, device="cuda"))
+    Tn = (25.0 + rng.uniform(-5, 30, (n, n, n))).astype(np.float32)
+    sc.T[par ^ 1].copy_(torch.as_tensor(Tn, device="cuda"))
+    plan.face_stage(dt)
+    torch.cuda.synchronize()
+    K = Kernels("f32")
+    af = [a.cpu().numpy() for a in (sc.ax, sc.ay, sc.az)]
+    kf = [np.ascontiguousarray(a, np.float32) for a in spec.static_k]
+    mf = [np.ascontiguousarray(a, np.float32) for a in spec.static_m]
+    outs = []
+    for axis in range(3):
+        o = np.zeros_like(uvw[axis])
+        K.call("or_advect_face", n, float(spec.h), dt, uvw[0], uvw[1], uvw[2], axis, uvw[axis], o)
+        outs.append(o)
+    K.call("or_buoyancy", n, dt, 9.81, float(spec.t_amb), outs[2], Tn)
+    for axis in range(3):
+        K.call("or_relax", n, float(spec.h), dt, float(spec.rho), float(spec.alpha_f_min), axis, outs[axis], kf[axis],
+               mf[axis], af[axis])
+    for nm, ref in zip("uvw", outs):
+        got = getattr(sc, nm)[par ^ 1].cpu().numpy()
+        assert np.array_equal(got.view(np.int32), ref.view(np.int32)), (nm, int((got != ref).sum()))
+    # temperature stage: blend (air-only: Tw = T), fixed cells, capped source, then the RK2 advection into T[par ^ 1]
+    T = (25.0 + rng.uniform(-5, 30, (n, n, n))).astype(np.float32)
+    sc.T[par].copy_(torch.as_tensor(T, device="cuda"))
+    plan.temperature_stage(dt)
+    torch.cuda.synchronize()
+    Tw = T.copy()
+    K.call("or_apply_fixed", n, Tw, np.ascontiguousarray(spec.fixed, np.int32), np.ascontiguousarray(spec.tfix, np.float32))
+    K.call("or_source", n, Tw, np.ascontiguousarray(spec.source, np.int32), float(spec.rate), float(spec.t_cap), dt)
+    T2 = np.zeros_like(T)
+    K.call("or_advect_T", n, float(spec.h), dt, Tw, np.ascontiguousarray(spec.static_alpha, np.float32), uvw[0], uvw[1],
+           uvw[2], T2)
+    got = sc.T[par ^ 1].cpu().numpy()
+    assert np.array_equal(got.view(np.int32), T2.view(np.int32)), int((got != T2).sum())
