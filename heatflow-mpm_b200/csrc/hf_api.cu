@@ -391,9 +391,11 @@ int hf_plan_upload(hf_plan* p, void* stream) {
         if (!sc.state) return fail(HF_ERR_ARG, "scene without a state block");
         const long long N = (long long)sc.n * sc.n * sc.n;
         for (long long f = 0; f < N; f += hf::kChunk) work.push_back(hf::WorkItem{s, (int)f});
-        for (int k0 = 0; k0 < sc.n; k0 += hf::kTK)
-            for (int j0 = 0; j0 < sc.n; j0 += hf::kTJ)
-                for (int i0 = 0; i0 < sc.n; i0 += hf::kTI) tiles.push_back(hf::TileItem{s, i0, j0, k0});
+        // k fastest, then i, then j: the six neighbours of a tile are at most (n / 32) (n / 4) tiles away in the
+        // table, so tiles solved side by side share their halo rows in L2
+        for (int j0 = 0; j0 < sc.n; j0 += hf::kTJ)
+            for (int i0 = 0; i0 < sc.n; i0 += hf::kTI)
+                for (int k0 = 0; k0 < sc.n; k0 += hf::kTK) tiles.push_back(hf::TileItem{s, i0, j0, k0});
     }
     begin[p->num_scenes] = (int)work.size();
     tbegin[p->num_scenes] = (int)tiles.size();

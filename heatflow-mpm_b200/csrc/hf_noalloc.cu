@@ -109,10 +109,10 @@ __global__ void k_noalloc_setup(hf_scene rec, unsigned char* base, ScratchLayout
     for (size_t b = tid; b < L.ws_bytes; b += stride) base[L.ws + b] = 0;
     hf::WorkItem* chunks = reinterpret_cast<hf::WorkItem*>(base + L.chunks);
     for (int c = tid; c < C; c += stride) chunks[c] = hf::WorkItem{0, c * hf::kChunk};
-    const int ti = (n + hf::kTI - 1) / hf::kTI, tj = (n + hf::kTJ - 1) / hf::kTJ;
+    const int ti = (n + hf::kTI - 1) / hf::kTI, tk = (n + hf::kTK - 1) / hf::kTK;
     hf::TileItem* tiles = reinterpret_cast<hf::TileItem*>(base + L.tiles);
-    for (int c = tid; c < T; c += stride)   // same order as hf_plan_upload: i fastest, then j, then k
-        tiles[c] = hf::TileItem{0, (c % ti) * hf::kTI, ((c / ti) % tj) * hf::kTJ, (c / (ti * tj)) * hf::kTK};
+    for (int c = tid; c < T; c += stride)   // same order as hf_plan_upload: k fastest, then i, then j
+        tiles[c] = hf::TileItem{0, ((c / tk) % ti) * hf::kTI, (c / (tk * ti)) * hf::kTJ, (c % tk) * hf::kTK};
     if (zero_q) {
         float* q = reinterpret_cast<float*>(base + L.qzero);
         const size_t NF = (size_t)(n + 1) * n * n;

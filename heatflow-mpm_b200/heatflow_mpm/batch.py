@@ -228,7 +228,10 @@ def autotune(batch: AirBatch, dt=2e-3, reps=3, candidates=None, cache=True):
         best = tuple(int(v) for v in table[key]["choice"])
         plan.plan.persistent_blocks, plan.plan.group_cells, plan.lanes = best
         return best, table[key]["timings"]
-    candidates = candidates or [(b * sms, g, l) for (g, l) in ((1, 1), (1, 2), (0, 1), (0, 2), (1, 4), (0, 4), (0, 8))
+    # group_cells: 0 = the library default (2.4 M cells), 1 = one scene per group, and sizes whose groups, times the
+    # lanes solving them side by side, keep the CG vectors (~40 B per cell) inside the 126 MB L2
+    candidates = candidates or [(b * sms, g, l) for (g, l) in ((1, 1), (1, 2), (0, 1), (0, 2), (1, 4), (0, 4), (0, 8),
+                                                               (600_000, 4), (1_200_000, 2), (800_000, 3))
                                 for b in (2, 4, 5)]
     timings = {}
     snap = batch.snapshot()
