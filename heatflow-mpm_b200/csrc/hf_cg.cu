@@ -1395,6 +1395,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     unsigned* bar = ws.bar + (HEAT ? 0 : kMaxLanes);
     unsigned epoch = 0;
     const float h = (float)S.h, hh = __fmul_rn(h, h), c_dt = __fdiv_rn((float)dt_d, hh);
+    const DivBy hhd = div_by(hh);
     double* bufA = ws.partA;
     double* bufB = ws.partB;
     const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
@@ -1597,7 +1598,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                         if (cl.k > 0) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk], __fsub_rn(pc, Pb[o - 1])));
                         if (cl.k < n - 1)
                             acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk + 1], __fsub_rn(pc, Pb[o + 1])));
-                        ap = __fdiv_rn(acc, hh);
+                        ap = div_rn(acc, hhd);
                     }
                     Apb[o] = ap;
                     pnew[cl.t] = pc;
@@ -1719,7 +1720,7 @@ constexpr int kPipeSlotFloats = kPipeCells + 3 * 1024;          // 9056 floats =
 // grid.py:94-115 k_laplacian of one tile cell from a staged box (centre offset o) and the tile's face boxes
 __device__ __forceinline__ float lap_box(const float* __restrict__ B, const float* __restrict__ axb,
                                          const float* __restrict__ ayb, const float* __restrict__ azb, const Cell& cl,
-                                         int n, int bi, int bj, int bk, int o, float hh) {
+                                         int n, int bi, int bj, int bk, int o, const DivBy& hh) {
     const float pc = B[o];
     float acc = 0.0f;
     if (cl.i > 0) acc = __fadd_rn(acc, __fmul_rn(axb[bi * 256 + bj * 32 + bk], __fsub_rn(pc, B[o - 400])));
@@ -1728,7 +1729,7 @@ __device__ __forceinline__ float lap_box(const float* __restrict__ B, const floa
     if (cl.j < n - 1) acc = __fadd_rn(acc, __fmul_rn(ayb[bi * 288 + (bj + 1) * 32 + bk], __fsub_rn(pc, B[o + 40])));
     if (cl.k > 0) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk], __fsub_rn(pc, B[o - 1])));
     if (cl.k < n - 1) acc = __fadd_rn(acc, __fmul_rn(azb[bi * 288 + bj * 36 + bk + 1], __fsub_rn(pc, B[o + 1])));
-    return __fdiv_rn(acc, hh);
+    return div_rn(acc, hh);
 }
 
 template <int MAXC>
@@ -1752,6 +1753,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     unsigned* bar = ws.bar + kMaxLanes;
     unsigned epoch = 0;
     const float h = (float)S.h, hh = __fmul_rn(h, h);
+    const DivBy hhd = div_by(hh);
     double* bufA = ws.partA;
     double* bufB = ws.partB;
     const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
@@ -1878,7 +1880,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 const int bj = lt >> 5, bk = lt & 31, o = (m + 1) * 400 + (bj + 1) * 40 + (bk + 4);
                 const float d = cells[2048 + e];
                 w[s] = lap_box(slot, slot + kPipeFaces, slot + kPipeFaces + kBX, slot + kPipeFaces + kBX + kBY, cl, n, m,
-                               bj, bk, o, hh);
+                               bj, bk, o, hhd);
                 const float u = __fmul_rn(d, r[s]);
                 mg1[cl.t] = __fmul_rn(d, w[s]);
                 part[0] += (double)r[s] * (double)u;
@@ -1948,7 +1950,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 if (!have[q] || !cl.ok) continue;
                 const int bj = lt >> 5, bk = lt & 31, o = (m + 1) * 400 + (bj + 1) * 40 + (bk + 4);
                 const float nv = lap_box(slot, slot + kPipeFaces, slot + kPipeFaces + kBX, slot + kPipeFaces + kBX + kBY,
-                                         cl, n, m, bj, bk, o, hh);
+                                         cl, n, m, bj, bk, o, hhd);
                 const float d = Dg[e];
                 const float u = __fmul_rn(d, r[s]);
                 z[s] = __fadd_rn(nv, __fmul_rn(beta, z[s]));

@@ -269,14 +269,14 @@ def test_divide_by_constant_matches_ieee(torch_cuda):
     Reference: the binary64 quotient of the two binary32 operands rounded to binary32 (double rounding is harmless for
     division when the intermediate has >= 2p + 2 bits).  Every binary32 value in [2^-12, 2^9) (both signs) and 16 M
     random bit patterns over the whole range (zeros, subnormals, infinities and NaNs included), for the cell sizes of
-    the test and benchmark scenes and the buoyancy denominator."""
+    the test and benchmark scenes, their squares (the CG stencils divide by h^2) and the buoyancy denominator."""
     torch = torch_cuda
     from heatflow_mpm import _lib
     L = _lib.load()
     L.hf_k_divide_by.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p]
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    divisors = {np.float32(v) for v in (0.01, 0.015, 0.005, 0.003, 0.02, 298.15)}
-    divisors |= {np.float32(0.48 / n) for n in (32, 48, 64, 96, 128, 160)}
+    hs = {np.float32(v) for v in (0.01, 0.015, 0.005, 0.003, 0.02)} | {np.float32(0.48 / n) for n in (32, 48, 64, 96, 128, 160)}
+    divisors = hs | {np.float32(h * h) for h in hs} | {np.float32(298.15)}   # h, h^2 (the CG stencils), buoyancy
     gen = torch.Generator(device="cuda").manual_seed(3)
     rnd = torch.randint(-2 ** 31, 2 ** 31 - 1, (1 << 24,), device="cuda", dtype=torch.int64, generator=gen).to(torch.int32)
     lo, hi = np.float32(2.0 ** -12).view(np.int32), np.float32(2.0 ** 9).view(np.int32)
