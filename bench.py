@@ -74,8 +74,9 @@ def parse():
                     help="plain: CG solves in the streaming kernel instead of the resident one")
     ap.add_argument("--persistent-blocks", type=int, default=0, help="plain: grid of the streaming CG kernel")
     ap.add_argument("--no-tma", action="store_true", help="plain: resident pressure CG without the TMA-staged stencil")
-    ap.add_argument("--cg", default="classic", choices=["classic", "pipelined"],
-                    help="plain: pressure solve by the classic or the pipelined (one barrier per iteration) Jacobi-PCG")
+    ap.add_argument("--cg", default="classic", choices=["classic", "single-reduction"],
+                    help="plain: pressure solve by the classic Jacobi-PCG or its single-reduction form (one grid "
+                         "barrier per iteration)")
     ap.add_argument("--scenes", type=int, default=64, help="batched: scenes in the ensemble")
     ap.add_argument("--graph-steps", type=int, default=10, help="batched: substeps per captured CUDA graph")
     ap.add_argument("--edges", default="32,48,64,96,128", help="batched: grid edges the ensemble draws from")

@@ -43,7 +43,7 @@ struct DeviceInfo {
     // occupancy of each resident variant [heat][tiles per group][tma][groups] (-1: not queried yet; the query also
     // raises the kernel's dynamic shared-memory limit)
     int res_occ[2][4][2][5];
-    int pipe_occ[4][5];   // the pipelined pressure variant [tiles per group][groups] (-1: not queried yet)
+    int pipe_occ[4][5];   // the single-reduction pressure variant [tiles per group][groups] (-1: not queried yet)
 };
 
 constexpr int kResGroupsMax[4] = {0, 4, 3, 2};   // 256-thread groups per block of the resident variant, by MAXC
@@ -105,10 +105,10 @@ Layout layout(int S, int C, int T) {
     o = align_up(o + sizeof(int) * (size_t)(S + 1), 256);
     L.maps = o;                      // kMapsPerScene TMA descriptors per scene (128 bytes each)
     o = align_up(o + sizeof(CUtensorMap) * hf::kMapsPerScene * (size_t)S, 256);
-    L.partA = o;
-    o = align_up(o + sizeof(double) * 3 * (size_t)T, 256);
+    L.partA = o;                     // 5 doubles per tile (3 used by the classic variants)
+    o = align_up(o + sizeof(double) * 5 * (size_t)T, 256);
     L.partB = o;
-    o = align_up(o + sizeof(double) * 3 * (size_t)T, 256);
+    o = align_up(o + sizeof(double) * 5 * (size_t)T, 256);
     L.mean_part = o;
     o = align_up(o + sizeof(double) * (size_t)C, 256);
     L.total = o;
@@ -235,13 +235,15 @@ int launch_resident(const hf_plan* p, DeviceInfo* d, bool heat, double dt, int s
     const bool tma = !(p->options & HF_PLAN_NO_TMA) &&
                      (heat ? (sc.n % 16 == 0 && sc.hkzc && sc.hkx && sc.hky && sc.cell_flags) : (sc.n % 4 == 0));
     const int want = (int)((p->options >> HF_PLAN_RES_TILES_SHIFT) & 3u);   // 0: the first that fits
-    // the pipelined pressure solve (one grid barrier per iteration) when the plan asks for it and the stencil is staged
-    const bool pipe = !heat && tma && (p->options & HF_PLAN_PIPELINED_CG);
+    // the single-reduction pressure solve (one grid barrier per iteration) when the plan asks for it, the stencil is
+    // staged and its scratch vectors exist
+    const bool pipe = !heat && tma && (p->options & HF_PLAN_SINGLE_REDUCTION_CG) && sc.cg_r && sc.cg_z && sc.cg_Ap &&
+                      sc.hdiag && sc.pdiag && sc.cg_p[0] && sc.cg_p[1];
     for (int m = want ? want : 1; m <= 3; ++m) {
         const int groups = (tpb + m - 1) / m;
         if (groups > kResGroupsMax[m]) continue;
-        const void* fn = pipe ? hf::pcg_pipe_kernel(m) : hf::pcg_resident_kernel(heat, m, tma);
-        const size_t smem = pipe ? hf::pcg_pipe_smem(groups, m) : hf::pcg_resident_smem(groups, m, tma, heat);
+        const void* fn = pipe ? hf::pcg_one_kernel(m) : hf::pcg_resident_kernel(heat, m, tma);
+        const size_t smem = pipe ? hf::pcg_one_smem(groups, m) : hf::pcg_resident_smem(groups, m, tma, heat);
         if (smem > d->smem_optin) continue;
         int& occ = pipe ? d->pipe_occ[m][groups] : d->res_occ[heat][m][tma][groups];
         if (occ < 0) {

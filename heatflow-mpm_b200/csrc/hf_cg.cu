@@ -162,6 +162,57 @@ __device__ __forceinline__ void scene_sums_wide(const double* __restrict__ buf, 
     }
 }
 
+// scene_sums for K components on G >= 3 groups of 256 threads (blockDim >= 768): group q sums components q, q + 3, ...
+// each exactly as scene_sums' first 256 threads do (the same tree, the same bits), with ceil(K / 3) of them per thread.
+template <int K, int STRIDE>
+__device__ __forceinline__ void scene_sums_3g(const double* __restrict__ buf, int b, int e, double (&tot)[K],
+                                              double* red) {
+    constexpr int KPT = (K + 2) / 3;
+    const int q = threadIdx.x >> 8, lt = threadIdx.x & 255;
+    double acc[KPT];
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) acc[j] = 0.0;
+    if (q < 3) {
+        int c = b + lt;
+        for (; c + 3 * kThreads < e; c += 4 * kThreads) {
+            double v[KPT][4];
+#pragma unroll
+            for (int j = 0; j < KPT; ++j)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) v[j][u] = q + 3 * j < K ? buf[STRIDE * (c + u * kThreads) + q + 3 * j] : 0.0;
+#pragma unroll
+            for (int j = 0; j < KPT; ++j)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[j] += v[j][u];
+        }
+        for (; c < e; c += kThreads) {
+#pragma unroll
+            for (int j = 0; j < KPT; ++j)
+                if (q + 3 * j < K) acc[j] += buf[STRIDE * c + q + 3 * j];
+        }
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+        }
+    }
+    const int lane = threadIdx.x & 31, wq = lt >> 5;
+    __syncthreads();
+    if (q < 3 && lane == 0) {
+#pragma unroll
+        for (int j = 0; j < KPT; ++j)
+            if (q + 3 * j < K) red[(q + 3 * j) * 32 + wq] = acc[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) s += red[c * 32 + w];
+        tot[c] = s;
+    }
+}
+
 // Per-256-thread-group sum (each group reduces its own 8 warps in index order): the tile partial tree.
 template <int K>
 __device__ __forceinline__ void group_sum(double (&v)[K], double* red) {
@@ -222,6 +273,28 @@ __device__ __forceinline__ void publish_group(const double* red, double* __restr
 #pragma unroll
                 for (int w = 0; w < 8; ++w) s += red[(3 * q + comp) * 32 + g0 + w];
                 buf[3 * c + comp] = s;
+            }
+        }
+    }
+}
+
+// publish_group for K components per tile at stride K (the single-reduction CG's five partials)
+template <int MAXC, int K>
+__device__ __forceinline__ void publish_k(const double* red, double* __restrict__ buf, int first_tile, int groups,
+                                          int c_end) {
+    __syncthreads();
+    if ((threadIdx.x & 255) == 0) {
+        const int g0 = (threadIdx.x >> 5);
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            const int c = first_tile + groups * q;
+            if (c >= c_end) continue;
+#pragma unroll
+            for (int comp = 0; comp < K; ++comp) {
+                double s = 0.0;
+#pragma unroll
+                for (int w = 0; w < 8; ++w) s += red[(K * q + comp) * 32 + g0 + w];
+                buf[K * c + comp] = s;
             }
         }
     }
@@ -1696,26 +1769,32 @@ finish:
     if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, HEAT, *(volatile int*)ws.err != 0, par);
 }
 
-// ====================================================================== resident pressure CG, one barrier per iteration
-// Pipelined Jacobi-PCG (Ghysels & Vanroose, "Hiding global synchronization latency in the preconditioned Conjugate
-// Gradient algorithm", Parallel Computing 40 (2014), Alg. 4) for the pressure system of one scene with n % 4 == 0.
-// In exact arithmetic it computes the iterates of the classic method above; its recurrences
-//     z = n + beta z,  s = w + beta s,  p = u + beta p,  x += alpha p,  r -= alpha s,  w -= alpha z
-// (u = D r, m = D w, n = A m, w = A u) need a scene sum only of gamma = r.u, delta = w.u and r.r, which are formed in the
-// same place as m, so the halo of m and the three partials are published before ONE grid barrier per iteration
-// (the classic method needs two: after p.Ap and after r.r / r.z).  alpha = gamma / (delta - beta gamma / alpha_old),
-// beta = gamma / gamma_old, in fp64 from the fixed-tree sums and rounded once; u and m are formed from r and w with the
-// diagonal (not by their own recurrences).  The convergence test is the classic one on the recursively updated
-// residual: r.r <= atol^2 with atol = max(tol ||b||, tol, 1e-18), tested before every update, so a converged solve
-// reports the same iteration count.  Rounding differs from the classic method (the vectors follow other
-// recurrences): results agree to ~1e-6 relative, not bit for bit.
+// ===================================================== resident pressure CG, one reduction point per iteration
+// Jacobi-PCG of the pressure system of one scene (n % 4 == 0) with ONE grid barrier per iteration instead of two.  The
+// vectors follow the classic recurrences exactly (A p formed from p every iteration, r -= alpha A p, z = D r,
+// p = z + beta p); only beta is obtained differently.  In iteration k every block forms, next to p_k . A p_k, the direct
+// r_k . r_k and r_k . z_k of its cells and the two terms A p_k . z_k and A p_k . D A p_k, so that one scene sum gives
+//     alpha_k = rz_k / pAp_k,   rz_{k+1} = rz_k - 2 alpha_k (A p_k . z_k) + alpha_k^2 (A p_k . D A p_k),
+//     beta_{k+1} = rz_{k+1} / rz_k
+// (the expansion of (r_k - alpha A p_k) . D (r_k - alpha A p_k) used by D'Azevedo, Eijkhout & Romine, "Conjugate
+// gradient algorithms with reduced synchronization overhead on distributed memory multiprocessors", 1993).  rz_k is
+// the direct sum of every iteration, so the expansion never accumulates; it differs from the direct rz_{k+1} only by
+// the binary32 rounding of r_{k+1} (~1e-7 relative), so beta moves by that much and the solve converges like the
+// classic one (the same iteration counts and x within ~1e-8 relative on the benchmark scene's systems; at tolerance
+// 1e-6 too).  The convergence test is the classic one on the direct r_k . r_k, taken at the barrier after r_k was
+// formed: a solve stops with the same x and reports the same iteration count.
 //
-// State: r, w, z, s of a thread's cells in registers; x, p and D of every tile cell in shared memory next to the
-// tile's boxes (the m box with a one-cell halo, restaged by TMA every iteration, and the face fractions, staged once).
-// m is double-buffered in global memory (cg_p[0], cg_p[1]): m_k is written during iteration k-1 and read during k.
-constexpr int kPipeFaces = kBZ;                                 // slot offset of the face-fraction boxes
-constexpr int kPipeCells = kBZ + kBX + kBY + kBW;               // slot offset of x, p, D (1024 floats each)
-constexpr int kPipeSlotFloats = kPipeCells + 3 * 1024;          // 9056 floats = 36,224 bytes (a multiple of 128)
+// Halo: the next iteration needs p_{k+1} at the tile's face neighbours, which belong to other blocks.  Every block
+// publishes r_k, A p_k and p_k of its cells (double-buffered: r in cg_r / cg_z, A p in cg_Ap / hdiag -- the heat
+// diagonal is dead while the pressure system is solved -- and p in cg_p[0] / cg_p[1]) and the Jacobi diagonal (pdiag);
+// after the barrier a block recomputes p_{k+1} = D (r_k - alpha A p_k) + beta p_k at its 832 face-neighbour points
+// with exactly the owner's operations, so the neighbours agree bit for bit.  State: r and p of a thread's cells in
+// registers; x, D and A p in shared memory beside the tile's p box (one-cell halo) and face-fraction boxes (staged
+// once by TMA).
+constexpr int kOneFaces = kBZ;                            // slot offset of the face-fraction boxes
+constexpr int kOneCells = kBZ + kBX + kBY + kBW;          // slot offset of x, D and A p (1024 floats each)
+constexpr int kOneSlotFloats = kOneCells + 3 * 1024;      // 9056 floats = 36,224 bytes (a multiple of 128)
+constexpr int kOneComps = 5;                              // partials per tile: pAp, rr, rz, Ap.z, Ap.D.Ap
 
 // grid.py:94-115 k_laplacian of one tile cell from a staged box (centre offset o) and the tile's face boxes
 __device__ __forceinline__ float lap_box(const float* __restrict__ B, const float* __restrict__ axb,
@@ -1732,16 +1811,38 @@ __device__ __forceinline__ float lap_box(const float* __restrict__ B, const floa
     return div_rn(acc, hh);
 }
 
+// Face-neighbour point q (0..3) of thread lt around a 4 x 8 x 32 tile, as box offsets (bi, bj, bk in -1..4, -1..8,
+// -1..32): the two i faces (256 points each), the two j faces (128 each) and the two k faces (32 each) -- 832 points,
+// three or four per thread, consecutive threads on consecutive k.  Returns false when the thread has no point q.
+__device__ __forceinline__ bool halo_point(int lt, int q, int& bi, int& bj, int& bk) {
+    if (q == 0 || q == 1) {
+        bi = q == 0 ? -1 : 4;
+        bj = lt >> 5;
+        bk = lt & 31;
+        return true;
+    }
+    if (q == 2) {
+        bi = (lt & 127) >> 5;
+        bj = lt < 128 ? -1 : 8;
+        bk = lt & 31;
+        return true;
+    }
+    if (lt >= 64) return false;
+    bi = (lt & 31) >> 3;
+    bj = lt & 7;
+    bk = lt < 32 ? -1 : 32;
+    return true;
+}
+
 template <int MAXC>
 __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
-    k_pcg_pipe(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int tile_lo, int tile_hi,
-               double dt_d, Workspace ws, const __grid_constant__ TileMaps maps) {
+    k_pcg_one(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int tile_lo, int tile_hi,
+              double dt_d, Workspace ws, const __grid_constant__ TileMaps maps) {
     constexpr int CPT = 4 * MAXC;
     extern __shared__ __align__(128) float sm_raw[];
     float* sm_slots = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
-    __shared__ double red[kRedComps * 32];
+    __shared__ double red[kOneComps * 3 * 32];   // five partials of up to three tiles per group, one per warp
     __shared__ LocalScene Ls;
-    __shared__ double s_gamma_old, s_alpha_old;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
     const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
     const int c0 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * blockIdx.x) / gridDim.x);
@@ -1754,12 +1855,17 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     unsigned epoch = 0;
     const float h = (float)S.h, hh = __fmul_rn(h, h);
     const DivBy hhd = div_by(hh);
-    double* bufA = ws.partA;
-    double* bufB = ws.partB;
+    double* const bufA = ws.partA;
+    double* const bufB = ws.partB;
     const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
     float* xg = S.p;
-    float* const mg0 = S.cg_p[0];
-    float* const mg1 = S.cg_p[1];
+    float* const Dg = S.pdiag;
+    float* const R0 = S.cg_r;
+    float* const R1 = S.cg_z;
+    float* const A0 = S.cg_Ap;
+    float* const A1 = S.hdiag;
+    float* const P0 = S.cg_p[0];
+    float* const P1 = S.cg_p[1];
     TileItem my[MAXC];
     bool have[MAXC];
 #pragma unroll
@@ -1768,38 +1874,16 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         have[q] = c < c1;
         my[q] = tiles[have[q] ? c : c0];
     }
-    auto slot_of = [&](int q) { return sm_slots + (size_t)(g * MAXC + q) * kPipeSlotFloats; };
-    // stage the m (or u) box of every own tile from buffer b; thread lt == 0 of the group issues
-    auto issue_box = [&](int b) {
-        if (lt == 0) {
-            asm volatile("fence.proxy.async.global;" ::: "memory");
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-#pragma unroll
-            for (int q = 0; q < MAXC; ++q) {
-                if (!have[q]) continue;
-                unsigned long long* mb = &mbar[g * MAXC + q];
-                mbar_expect_tx(mb, (unsigned)(kBZ * sizeof(float)));
-                tma_load_3d(slot_of(q), b ? &maps.p1 : &maps.p0, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
-            }
-        }
-    };
-    unsigned phase_bit = 0;
-    auto wait_boxes = [&]() {
-        bool ok = true;
-#pragma unroll
-        for (int q = 0; q < MAXC; ++q)
-            if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], phase_bit) && ok;
-        if (!ok) atomicExch(ws.err, 1);
-        phase_bit ^= 1u;
-    };
+    auto slot_of = [&](int q) { return sm_slots + (size_t)(g * MAXC + q) * kOneSlotFloats; };
     if (lt == 0) {
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) mbar_init(&mbar[g * MAXC + q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    float r[CPT], w[CPT], z[CPT], sv[CPT];
+    float r[CPT], pv[CPT];
     int k = 0;
+    bool faces_requested = false;
     // ------------------------------------------------------------------------------------------ set-up
     float mean = 0.0f;
     {
@@ -1809,29 +1893,31 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         mean = __double2float_rn(mm[0] / ((double)n * n * n));
     }
     {
-        // r0 = b - A x0, u0 = D r0 (published for the halo of w0 = A u0); partials b.b, r.r, r.u
+        // r0 = b - A x0, z0 = D r0, p0 = z0 (published for the halo of A p0); partials b.b, r.r, r.z
         __syncthreads();   // red is free (the rhs mean above read it)
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) {
             double part[3] = {0.0, 0.0, 0.0};
-            float* cells = slot_of(q) + kPipeCells;
+            float* cells = slot_of(q) + kOneCells;
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
                 const int s = q * 4 + m, e = m * 256 + lt;
-                r[s] = w[s] = z[s] = sv[s] = 0.0f;
+                r[s] = pv[s] = 0.0f;
                 cells[e] = cells[1024 + e] = cells[2048 + e] = 0.0f;
                 const Cell cl = tile_cell(my[q], n, lt, m);
                 if (!have[q] || !cl.ok) continue;
                 float b, d, rr;
                 setup_cell<false>(S, xg, mean, hh, 0.0f, cl, b, d, rr);
-                const float u = __fmul_rn(d, rr);
+                const float z = __fmul_rn(d, rr);
                 cells[e] = xg[cl.t];
-                cells[2048 + e] = d;
+                cells[1024 + e] = d;
+                Dg[cl.t] = d;
                 r[s] = rr;
-                mg0[cl.t] = u;
+                pv[s] = z;
+                P0[cl.t] = z;
                 part[0] += (double)b * (double)b;
                 part[1] += (double)rr * (double)rr;
-                part[2] += (double)rr * (double)u;
+                part[2] += (double)rr * (double)z;
             }
             stash_warp<3>(part, red, 3 * q);
         }
@@ -1845,12 +1931,20 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             float* slot = slot_of(q);
             unsigned long long* mb = &mbar[g * MAXC + q];
             mbar_expect_tx(mb, (unsigned)((kBX + kBY + kBW) * sizeof(float)));
-            tma_load_3d(slot + kPipeFaces, &maps.ax, my[q].k0, my[q].j0, my[q].i0, mb);
-            tma_load_3d(slot + kPipeFaces + kBX, &maps.ayc, my[q].k0, my[q].j0, my[q].i0, mb);
-            tma_load_3d(slot + kPipeFaces + kBX + kBY, &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + kOneFaces, &maps.ax, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + kOneFaces + kBX, &maps.ayc, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + kOneFaces + kBX + kBY, &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
         }
     }
-    wait_boxes();
+    faces_requested = true;
+    {
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], 0) && ok;
+        if (!ok) atomicExch(ws.err, 1);
+    }
+    faces_requested = false;
     if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
     {
         double tot[3];
@@ -1863,119 +1957,151 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         __syncthreads();
     }
     if (!Ls.live) goto writeback;
-    {
-        // w0 = A u0 from the staged u0 boxes; partials of iteration 0 (r.u, w.u, r.r); m0 = D w0 published
-        issue_box(0);
-        wait_boxes();
-#pragma unroll
-        for (int q = 0; q < MAXC; ++q) {
-            double part[3] = {0.0, 0.0, 0.0};
-            const float* slot = slot_of(q);
-            const float* cells = slot + kPipeCells;
-#pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                const int s = q * 4 + m, e = m * 256 + lt;
-                const Cell cl = tile_cell(my[q], n, lt, m);
-                if (!have[q] || !cl.ok) continue;
-                const int bj = lt >> 5, bk = lt & 31, o = (m + 1) * 400 + (bj + 1) * 40 + (bk + 4);
-                const float d = cells[2048 + e];
-                w[s] = lap_box(slot, slot + kPipeFaces, slot + kPipeFaces + kBX, slot + kPipeFaces + kBX + kBY, cl, n, m,
-                               bj, bk, o, hhd);
-                const float u = __fmul_rn(d, r[s]);
-                mg1[cl.t] = __fmul_rn(d, w[s]);
-                part[0] += (double)r[s] * (double)u;
-                part[1] += (double)w[s] * (double)u;
-                part[2] += (double)r[s] * (double)r[s];
-            }
-            stash_warp<3>(part, red, 3 * q);
-        }
-        publish_group<MAXC>(red, bufA, c0 + g, groups, c1);
-    }
-    if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
     // ------------------------------------------------------------------------------------------ iterations
+    // k = 0 forms A p0 from the published p0; k >= 1 first advances x, r and p with the scalars of iteration k - 1
     for (k = 0;; ++k) {
-        // m_k lives in buffer (k + 1) & 1: request its boxes first, so that the copy overlaps the scene sums
-        issue_box((k + 1) & 1);
-        {
-            double tot[3];
-            const int comp[3] = {0, 1, 2};
-            if (MAXC < 3 && blockDim.x >= 3 * kThreads)   // each component on its own 256 threads
-                scene_sums_wide<3>((k & 1) ? bufB : bufA, cb, ce, 0, tot, red);
-            else
-                scene_sums<3>((k & 1) ? bufB : bufA, cb, ce, comp, tot, red);
+        const int cur = k & 1, prev = cur ^ 1;
+        float alpha = 0.0f, beta = 0.0f;
+        // the halo of p_k: the neighbours' published values, loaded right after the barrier
+        float hr[4], ha[4], hp[4], hd[4];
+        if (k > 0) {
+            double tot[kOneComps];
+            // pAp, rr, rz, Ap.z, Ap.D.Ap of iteration k - 1
+            if (MAXC < 3 && blockDim.x >= 3 * kThreads) {
+                scene_sums_3g<kOneComps, kOneComps>(prev ? bufB : bufA, cb, ce, tot, red);
+            } else {
+                const int comp[kOneComps] = {0, 1, 2, 3, 4};
+                scene_sums<kOneComps, kOneComps>(prev ? bufB : bufA, cb, ce, comp, tot, red);
+            }
             if (threadIdx.x == 0) {
-                // tot = (gamma_k, delta_k, r_k.r_k); the classic test on r_k before the update of iteration k + 1
-                const double gamma = tot[0], delta = tot[1], rr = tot[2];
-                Ls.iters = k;
+                // the classic test on r_{k-1} (formed in iteration k - 1): converged -> x_{k-1} is the solution
+                const double pAp = tot[0], rr = tot[1], rz = tot[2];
+                Ls.iters = k - 1;
                 Ls.rr = rr;
-                Ls.rz = gamma;
+                Ls.rz = rz;
+                Ls.pAp = pAp;
                 const bool above = rr > Ls.atol_sq;
                 if (!isfinite(rr)) Ls.status |= HF_SCENE_NONFINITE;
-                const bool live = above && isfinite(rr) && k < Ls.maxit;
+                const bool live = above && isfinite(rr) && (k - 1) < Ls.maxit;
                 if (!live && above && isfinite(rr)) Ls.status |= HF_SCENE_PRESSURE_MAXITER;
                 Ls.live = live;
                 if (live) {
-                    double alpha, beta;
-                    if (k == 0) {
-                        beta = 0.0;
-                        alpha = gamma / delta;
-                    } else {
-                        beta = gamma / s_gamma_old;
-                        alpha = gamma / (delta - beta * gamma / s_alpha_old);
-                    }
-                    s_gamma_old = gamma;
-                    s_alpha_old = alpha;
-                    Ls.alpha = __double2float_rn(alpha);
-                    Ls.beta = __double2float_rn(beta);
-                    Ls.pAp = delta;
+                    const double a = rz / pAp;
+                    const double rz_next = rz - 2.0 * a * tot[3] + a * a * tot[4];
+                    Ls.alpha = __double2float_rn(a);
+                    Ls.beta = __double2float_rn(rz_next / rz);
                 }
             }
             __syncthreads();
+            if (!Ls.live) break;
+            alpha = Ls.alpha;
+            beta = Ls.beta;
         }
-        wait_boxes();
-        if (!Ls.live) break;
-        const float alpha = Ls.alpha, beta = Ls.beta;
-        float* mnext = (k & 1) ? mg1 : mg0;   // m_{k+1}
+        // p_k in every tile's box: own cells from registers, face neighbours recomputed from their published values
+        {
+            const float* Rp = prev ? R1 : R0;
+            const float* Ap_ = prev ? A1 : A0;
+            const float* Pp = prev ? P1 : P0;
 #pragma unroll
-        for (int q = 0; q < MAXC; ++q) {
-            double part[3] = {0.0, 0.0, 0.0};
-            const float* slot = slot_of(q);
-            float* X = slot_of(q) + kPipeCells;
-            float* P = X + 1024;
-            const float* Dg = X + 2048;
+            for (int q = 0; q < MAXC; ++q) {
+                float* box = slot_of(q);
+                int ho[4];
 #pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                const int s = q * 4 + m, e = m * 256 + lt;
-                const Cell cl = tile_cell(my[q], n, lt, m);
-                if (!have[q] || !cl.ok) continue;
-                const int bj = lt >> 5, bk = lt & 31, o = (m + 1) * 400 + (bj + 1) * 40 + (bk + 4);
-                const float nv = lap_box(slot, slot + kPipeFaces, slot + kPipeFaces + kBX, slot + kPipeFaces + kBX + kBY,
-                                         cl, n, m, bj, bk, o, hhd);
-                const float d = Dg[e];
-                const float u = __fmul_rn(d, r[s]);
-                z[s] = __fadd_rn(nv, __fmul_rn(beta, z[s]));
-                sv[s] = __fadd_rn(w[s], __fmul_rn(beta, sv[s]));
-                const float pk = __fadd_rn(u, __fmul_rn(beta, P[e]));
-                P[e] = pk;
-                X[e] = __fadd_rn(X[e], __fmul_rn(alpha, pk));
-                r[s] = __fsub_rn(r[s], __fmul_rn(alpha, sv[s]));
-                w[s] = __fsub_rn(w[s], __fmul_rn(alpha, z[s]));
-                const float un = __fmul_rn(d, r[s]);
-                mnext[cl.t] = __fmul_rn(d, w[s]);
-                part[0] += (double)r[s] * (double)un;
-                part[1] += (double)w[s] * (double)un;
-                part[2] += (double)r[s] * (double)r[s];
+                for (int u = 0; u < 4; ++u) {
+                    int bi = 0, bj = 0, bk = 0;
+                    ho[u] = -1;
+                    if (!have[q] || !halo_point(lt, u, bi, bj, bk)) continue;
+                    const int gi = my[q].i0 + bi, gj = my[q].j0 + bj, gk = my[q].k0 + bk;
+                    if (gi < 0 || gi >= n || gj < 0 || gj >= n || gk < 0 || gk >= n) continue;
+                    ho[u] = (gi * n + gj) * n + gk;
+                }
+                // k = 0: p0 itself (published in the set-up, buffer 0); k >= 1: D (r - alpha Ap) + beta p
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int t = ho[u];
+                    if (t < 0) continue;
+                    if (k == 0) {
+                        hp[u] = P0[t];
+                    } else {
+                        hr[u] = Rp[t];
+                        ha[u] = Ap_[t];
+                        hp[u] = Pp[t];
+                        hd[u] = Dg[t];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int t = ho[u];
+                    if (t < 0) continue;
+                    int bi = 0, bj = 0, bk = 0;
+                    halo_point(lt, u, bi, bj, bk);
+                    float pk = hp[u];
+                    if (k > 0)
+                        pk = __fadd_rn(__fmul_rn(hd[u], __fsub_rn(hr[u], __fmul_rn(alpha, ha[u]))), __fmul_rn(beta, pk));
+                    box[(bi + 1) * 400 + (bj + 1) * 40 + (bk + 4)] = pk;
+                }
+                float* X = slot_of(q) + kOneCells;
+                const float* Dc = X + 1024;
+                const float* Apc = X + 2048;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int s = q * 4 + m, e = m * 256 + lt;
+                    const Cell cl = tile_cell(my[q], n, lt, m);
+                    if (!have[q] || !cl.ok) continue;
+                    if (k > 0) {
+                        // x_k = x_{k-1} + alpha p_{k-1}; r_k = r_{k-1} - alpha A p_{k-1}; p_k = D r_k + beta p_{k-1}
+                        X[e] = __fadd_rn(X[e], __fmul_rn(alpha, pv[s]));
+                        r[s] = __fsub_rn(r[s], __fmul_rn(alpha, Apc[e]));
+                        pv[s] = __fadd_rn(__fmul_rn(Dc[e], r[s]), __fmul_rn(beta, pv[s]));
+                    }
+                    box[(m + 1) * 400 + ((lt >> 5) + 1) * 40 + ((lt & 31) + 4)] = pv[s];
+                }
             }
-            stash_warp<3>(part, red, 3 * q);
         }
-        publish_group<MAXC>(red, (k & 1) ? bufA : bufB, c0 + g, groups, c1);   // partials of iteration k + 1
+        asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory");
+        // A p_k from the box; partials of iteration k; publish r_k, A p_k, p_k for the neighbours' next halo
+        {
+            float* const Rc = cur ? R1 : R0;
+            float* const Ac = cur ? A1 : A0;
+            float* const Pc = cur ? P1 : P0;
+            __syncthreads();   // red is free (the scene sums above read it)
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                double part[kOneComps] = {0.0, 0.0, 0.0, 0.0, 0.0};
+                const float* slot = slot_of(q);
+                const float* Dc = slot + kOneCells + 1024;
+                float* Apc = slot_of(q) + kOneCells + 2048;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int s = q * 4 + m, e = m * 256 + lt;
+                    const Cell cl = tile_cell(my[q], n, lt, m);
+                    if (!have[q] || !cl.ok) continue;
+                    const int bj = lt >> 5, bk = lt & 31, o = (m + 1) * 400 + (bj + 1) * 40 + (bk + 4);
+                    const float apv = lap_box(slot, slot + kOneFaces, slot + kOneFaces + kBX, slot + kOneFaces + kBX + kBY,
+                                              cl, n, m, bj, bk, o, hhd);
+                    Apc[e] = apv;
+                    const double d = Dc[e], a = apv, rs = r[s];
+                    const double z = __fmul_rn(Dc[e], r[s]);
+                    part[0] += (double)pv[s] * a;
+                    part[1] += rs * rs;
+                    part[2] += rs * z;
+                    part[3] += a * z;
+                    part[4] += a * (d * a);
+                    Rc[cl.t] = r[s];
+                    Ac[cl.t] = apv;
+                    Pc[cl.t] = pv[s];
+                }
+                stash_warp<kOneComps>(part, red, kOneComps * q);
+            }
+            publish_k<MAXC, kOneComps>(red, cur ? bufB : bufA, c0 + g, groups, c1);
+        }
         if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
     }
 writeback:
     // -------------------------------------------------- write x back, then project the faces
 #pragma unroll
     for (int q = 0; q < MAXC; ++q) {
-        const float* X = slot_of(q) + kPipeCells;
+        const float* X = slot_of(q) + kOneCells;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             const Cell cl = tile_cell(my[q], n, lt, m);
@@ -1987,7 +2113,7 @@ writeback:
         const float dtr = (float)(dt_d / S.rho);
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) {
-            const float* X = slot_of(q) + kPipeCells;
+            const float* X = slot_of(q) + kOneCells;
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
                 const Cell cl = tile_cell(my[q], n, lt, m);
@@ -1997,23 +2123,22 @@ writeback:
         }
     }
 finish:
-    if (*(volatile int*)ws.err) {
-        // leave no copy in flight: the last requested boxes are waited for again (bounded) before the block exits
-        // (every request is waited for before the next barrier, so only a wait that gave up can leave one)
+    if (*(volatile int*)ws.err || faces_requested) {
+        // leave no copy in flight: the face boxes are waited for again (bounded) before the block exits
 #pragma unroll
         for (int q = 0; q < MAXC; ++q)
-            if (have[q]) mbar_wait(&mbar[g * MAXC + q], phase_bit ^ 1u);
+            if (have[q]) mbar_wait(&mbar[g * MAXC + q], 0);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, false, *(volatile int*)ws.err != 0, par);
 }
 
-const void* pcg_pipe_kernel(int maxc) {
-    if (maxc == 1) return (const void*)k_pcg_pipe<1>;
-    if (maxc == 2) return (const void*)k_pcg_pipe<2>;
-    return (const void*)k_pcg_pipe<3>;
+const void* pcg_one_kernel(int maxc) {
+    if (maxc == 1) return (const void*)k_pcg_one<1>;
+    if (maxc == 2) return (const void*)k_pcg_one<2>;
+    return (const void*)k_pcg_one<3>;
 }
 
-size_t pcg_pipe_smem(int groups, int maxc) { return (size_t)groups * maxc * kPipeSlotFloats * sizeof(float) + 128; }
+size_t pcg_one_smem(int groups, int maxc) { return (size_t)groups * maxc * kOneSlotFloats * sizeof(float) + 128; }
 
 const void* pcg_kernel(bool heat, bool tma) {
     return heat ? (const void*)k_pcg<true, false> : tma ? (const void*)k_pcg<false, true> : (const void*)k_pcg<false, false>;

@@ -74,10 +74,11 @@ size_t pcg_stream_smem(bool tma);
 // scene's tiles; the TileMaps is used when tma; dynamic shared memory pcg_resident_smem(...)
 const void* pcg_resident_kernel(bool heat, int maxc, bool tma);
 size_t pcg_resident_smem(int groups, int maxc, bool tma, bool heat);
-// pipelined register-resident pressure solve of one scene with n % 4 == 0 (one grid barrier per CG iteration), the
-// same arguments and thread layout as the TMA resident variant; dynamic shared memory pcg_pipe_smem(groups, maxc)
-const void* pcg_pipe_kernel(int maxc);
-size_t pcg_pipe_smem(int groups, int maxc);
+// single-reduction register-resident pressure solve of one scene with n % 4 == 0 (one grid barrier per CG iteration;
+// uses hdiag as scratch), the same arguments and thread layout as the TMA resident variant; dynamic shared memory
+// pcg_one_smem(groups, maxc)
+const void* pcg_one_kernel(int maxc);
+size_t pcg_one_smem(int groups, int maxc);
 // limit of the CG kernels' bounded waits on the current device and the block kept from the first grid barrier
 // (-1: none); synchronous (constant memory)
 int set_wait_limit(unsigned long long limit_ns, int absent_block);

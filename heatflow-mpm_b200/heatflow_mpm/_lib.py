@@ -20,7 +20,7 @@ CHUNK = 1024
 HF_PLAN_STREAMING_CG = 1
 HF_PLAN_NO_TMA = 2
 HF_PLAN_STREAMING_HEAT = 4
-HF_PLAN_PIPELINED_CG = 8
+HF_PLAN_SINGLE_REDUCTION_CG = 8
 HF_PLAN_LANES_SHIFT = 8
 HF_PLAN_RES_TILES_SHIFT = 12
 

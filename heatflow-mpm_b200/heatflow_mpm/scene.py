@@ -296,17 +296,18 @@ class ScenePlan:
         self.plan.options = (self.plan.options & ~(3 << _lib.HF_PLAN_RES_TILES_SHIFT)) | (int(m) << _lib.HF_PLAN_RES_TILES_SHIFT)
 
     @property
-    def pipelined_cg(self):
-        """Pressure solve of a single-scene plan (n % 4 == 0) by pipelined Jacobi-PCG: one grid barrier per iteration,
-        the same stopping rule, rounding that differs from the classic method by ~1e-6 relative.  Off by default."""
-        return bool(self.plan.options & _lib.HF_PLAN_PIPELINED_CG)
+    def single_reduction_cg(self):
+        """Pressure solve of a single-scene plan (n % 4 == 0) with one grid barrier per CG iteration: the classic
+        vector recurrences, beta from the expansion of the next r.z in the iteration's partials, the classic stopping
+        test; results within ~1e-6 relative of the classic method.  Off by default."""
+        return bool(self.plan.options & _lib.HF_PLAN_SINGLE_REDUCTION_CG)
 
-    @pipelined_cg.setter
-    def pipelined_cg(self, on):
+    @single_reduction_cg.setter
+    def single_reduction_cg(self, on):
         if on:
-            self.plan.options |= _lib.HF_PLAN_PIPELINED_CG
+            self.plan.options |= _lib.HF_PLAN_SINGLE_REDUCTION_CG
         else:
-            self.plan.options &= ~_lib.HF_PLAN_PIPELINED_CG
+            self.plan.options &= ~_lib.HF_PLAN_SINGLE_REDUCTION_CG
 
     def stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)

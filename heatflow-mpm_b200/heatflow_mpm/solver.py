@@ -5,8 +5,9 @@ Same constructor, methods and attributes as the reference.  One extra keyword, `
 and velocities; used when Newton is not installed) or a body object of the caller's (``mpm.DLPackBody`` interface).  The air substep itself -- obstacle fields, temperature stages,
 heat CG, FLIP particle update, face stage, pressure CG and projection -- is one call into libheatflow_b200, replayed
 from a CUDA graph after the first substep at each dt (``graph=False``: launched directly every time; same bits).
-``cg="pipelined"`` solves the pressure system by pipelined Jacobi-PCG (one grid barrier per iteration instead of two;
-the same stopping rule; results within ~1e-6 relative of the classic method, which stays the default)."""
+``cg="single-reduction"`` solves the pressure system with one grid barrier per CG iteration instead of two (the classic
+recurrences with beta from an expansion of the next r.z; the same stopping test; results within ~1e-6 relative of the
+classic method, which stays the default)."""
 from __future__ import annotations
 
 from dataclasses import asdict
@@ -75,9 +76,9 @@ class HeatflowMPM:
         with torch.cuda.device(torch.device(device)):
             self.scene = DeviceScene(spec, device)
             self.plan = ScenePlan([self.scene], device, persistent_blocks=persistent_blocks)
-            if cg not in ("classic", "pipelined"):
-                raise ValueError("cg must be 'classic' or 'pipelined'")
-            self.plan.pipelined_cg = cg == "pipelined"
+            if cg not in ("classic", "single-reduction"):
+                raise ValueError("cg must be 'classic' or 'single-reduction'")
+            self.plan.single_reduction_cg = cg == "single-reduction"
             self.plan.prepare_statics()
         self.grid._bind(self.scene, self.plan, 0)
         self.heat._bind(self.scene)

@@ -122,11 +122,12 @@ typedef struct hf_scene {
                                         the scene's tiles fit one block per SM) */
 #define HF_PLAN_NO_TMA 2u            /* resident pressure CG without the TMA-staged stencil */
 #define HF_PLAN_STREAMING_HEAT 4u    /* the heat CG of a single-scene plan in the streaming kernel (pressure unchanged) */
-#define HF_PLAN_PIPELINED_CG 8u      /* single-scene plans with n % 4 == 0: the pressure solve by pipelined Jacobi-PCG
-                                        (Ghysels & Vanroose 2014; one grid barrier per iteration instead of two).  Same
-                                        stopping rule (r.r <= atol^2 on the recursive residual) and, in exact
-                                        arithmetic, the same iterates; the binary32 rounding differs from the classic
-                                        method (agreement ~1e-6 relative), so it is off by default. */
+#define HF_PLAN_SINGLE_REDUCTION_CG 8u /* single-scene plans with n % 4 == 0: the pressure solve with one grid barrier
+                                          per CG iteration instead of two -- the classic vector recurrences, beta from
+                                          the expansion of the next r.z in the iteration's partials (D'Azevedo,
+                                          Eijkhout & Romine 1993), the classic stopping test; results within ~1e-6
+                                          relative of the classic method, so it is off by default.  Uses the scene's
+                                          hdiag as scratch during the pressure solve. */
 #define HF_PLAN_MAPS_READY 0x8000u   /* set by hf_plan_upload: the workspace holds the scenes' TMA descriptors (the
                                         streaming pressure CG stages its stencil boxes with TMA when every active scene
                                         has n % 4 == 0) */

@@ -41,15 +41,15 @@ def _plain(n=32, seed=3, **spec_kw):
     return sc, plan
 
 
-@pytest.mark.parametrize("variant", ["resident", "pipelined", "streaming"])
+@pytest.mark.parametrize("variant", ["resident", "single-reduction", "streaming"])
 def test_maxiter_is_reported(torch_cuda, variant):
     """cg_max_iter = 1 (run as 2: warp's iterations come in pairs) cannot reach tol 1e-4 from a random velocity field:
     the pressure solve stops at 2 iterations and sets HF_SCENE_PRESSURE_MAXITER; a heat tolerance of 1e-14 with
     heat_maxiter = 1 sets HF_SCENE_HEAT_MAXITER."""
     from heatflow_mpm import _lib
     sc, plan = _plain(cg_max_iter=1, heat_maxiter=1, heat_tol=1e-14)
-    if variant == "pipelined":
-        plan.pipelined_cg = True
+    if variant == "single-reduction":
+        plan.single_reduction_cg = True
     elif variant == "streaming":
         plan.plan.options |= _lib.HF_PLAN_STREAMING_CG
     plan.substep(DT)
@@ -90,7 +90,7 @@ def test_nonfinite_scene_is_flagged_alone(torch_cuda):
             assert np.array_equal(s.current(nm).cpu().numpy(), ref[nm]), nm
 
 
-@pytest.mark.parametrize("variant", ["resident", "pipelined", "batch"])
+@pytest.mark.parametrize("variant", ["resident", "single-reduction", "batch"])
 def test_barrier_timeout_is_reported_and_the_device_stays_usable(torch_cuda, variant):
     """A wait limit of 1 ms and block 0 kept from the first grid barrier of every CG launch: the barrier cannot
     complete, every other block gives up after the limit, the launch returns and the scene's status carries
@@ -105,7 +105,7 @@ def test_barrier_timeout_is_reported_and_the_device_stays_usable(torch_cuda, var
         scenes, plan = batch.scenes, batch.plan
     else:
         sc, plan = _plain()
-        plan.pipelined_cg = variant == "pipelined"
+        plan.single_reduction_cg = variant == "single-reduction"
         scenes = [sc]
     par0 = [s.read_state().parity for s in scenes]
     torch.cuda.synchronize()
