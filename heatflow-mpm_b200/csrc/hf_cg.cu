@@ -1771,8 +1771,8 @@ finish:
 
 // ===================================================== resident pressure CG, one reduction point per iteration
 // Jacobi-PCG of the pressure system of one scene (n % 4 == 0) with ONE grid barrier per iteration instead of two.  The
-// vectors follow the classic recurrences exactly (A p formed from p every iteration, r -= alpha A p, z = D r,
-// p = z + beta p); only beta is obtained differently.  In iteration k every block forms, next to p_k . A p_k, the direct
+// vectors follow the classic recurrences (A p formed from p every iteration, r -= alpha A p, p = z + beta p with
+// z ~ D r); only beta is obtained differently.  In iteration k every block forms, next to p_k . A p_k, the direct
 // r_k . r_k and r_k . z_k of its cells and the two terms A p_k . z_k and A p_k . D A p_k, so that one scene sum gives
 //     alpha_k = rz_k / pAp_k,   rz_{k+1} = rz_k - 2 alpha_k (A p_k . z_k) + alpha_k^2 (A p_k . D A p_k),
 //     beta_{k+1} = rz_{k+1} / rz_k
@@ -1784,17 +1784,21 @@ finish:
 // 1e-6 too).  The convergence test is the classic one on the direct r_k . r_k, taken at the barrier after r_k was
 // formed: a solve stops with the same x and reports the same iteration count.
 //
-// Halo: the next iteration needs p_{k+1} at the tile's face neighbours, which belong to other blocks.  Every block
-// publishes r_k, A p_k and p_k of its cells (double-buffered: r in cg_r / cg_z, A p in cg_Ap / hdiag -- the heat
-// diagonal is dead while the pressure system is solved -- and p in cg_p[0] / cg_p[1]) and the Jacobi diagonal (pdiag);
-// after the barrier a block recomputes p_{k+1} = D (r_k - alpha A p_k) + beta p_k at its 832 face-neighbour points
-// with exactly the owner's operations, so the neighbours agree bit for bit.  State: r and p of a thread's cells in
-// registers; x, D and A p in shared memory beside the tile's p box (one-cell halo) and face-fraction boxes (staged
-// once by TMA).
+// Halo: iteration k + 1 needs p_{k+1} = z_{k+1} + beta p_k at the tile's face neighbours, which belong to other
+// blocks.  Every block publishes, for its cells, p_k, z_k' = D r_k and q_k = D A p_k (double-buffered: p in cg_p[0] /
+// cg_p[1], z' in cg_r / cg_z, q in cg_Ap / hdiag -- the heat diagonal is dead while the pressure system is solved).
+// Right after the barrier a block requests its tiles' p_k boxes (TMA) and the z', q values of their 832 face-neighbour
+// points (cp.async), both in flight while it sums the partials; then every p_{k+1} in its boxes, own cells and
+// neighbours alike, is formed by the same operations, z = z' - alpha q, p = z + beta p, so all blocks agree bit for
+// bit.  State: r, A p and D of a thread's cells in registers; x, the p box (one-cell halo), the face-fraction boxes
+// (TMA, once) and the halo staging in shared memory.
 constexpr int kOneFaces = kBZ;                            // slot offset of the face-fraction boxes
-constexpr int kOneCells = kBZ + kBX + kBY + kBW;          // slot offset of x, D and A p (1024 floats each)
-constexpr int kOneSlotFloats = kOneCells + 3 * 1024;      // 9056 floats = 36,224 bytes (a multiple of 128)
+constexpr int kOneCells = kBZ + kBX + kBY + kBW;          // slot offset of x (1024 floats)
+constexpr int kOneHalo = kOneCells + 1024;                // slot offset of the halo staging: z' and q of 832 points
+constexpr int kOneHaloPts = 832;
+constexpr int kOneSlotFloats = kOneHalo + 2 * kOneHaloPts;   // 8672 floats = 34,688 bytes (a multiple of 128)
 constexpr int kOneComps = 5;                              // partials per tile: pAp, rr, rz, Ap.z, Ap.D.Ap
+static_assert(kOneSlotFloats % 32 == 0, "slots stay 128-byte aligned");
 
 // grid.py:94-115 k_laplacian of one tile cell from a staged box (centre offset o) and the tile's face boxes
 __device__ __forceinline__ float lap_box(const float* __restrict__ B, const float* __restrict__ axb,
@@ -1811,17 +1815,18 @@ __device__ __forceinline__ float lap_box(const float* __restrict__ B, const floa
     return div_rn(acc, hh);
 }
 
-// Face-neighbour point q (0..3) of thread lt around a 4 x 8 x 32 tile, as box offsets (bi, bj, bk in -1..4, -1..8,
+// Face-neighbour point u (0..3) of thread lt around a 4 x 8 x 32 tile, as box offsets (bi, bj, bk in -1..4, -1..8,
 // -1..32): the two i faces (256 points each), the two j faces (128 each) and the two k faces (32 each) -- 832 points,
-// three or four per thread, consecutive threads on consecutive k.  Returns false when the thread has no point q.
-__device__ __forceinline__ bool halo_point(int lt, int q, int& bi, int& bj, int& bk) {
-    if (q == 0 || q == 1) {
-        bi = q == 0 ? -1 : 4;
+// three or four per thread, consecutive threads on consecutive k; staging index u * 256 + lt.  False when the thread
+// has no point u.
+__device__ __forceinline__ bool halo_point(int lt, int u, int& bi, int& bj, int& bk) {
+    if (u == 0 || u == 1) {
+        bi = u == 0 ? -1 : 4;
         bj = lt >> 5;
         bk = lt & 31;
         return true;
     }
-    if (q == 2) {
+    if (u == 2) {
         bi = (lt & 127) >> 5;
         bj = lt < 128 ? -1 : 8;
         bk = lt & 31;
@@ -1832,6 +1837,19 @@ __device__ __forceinline__ bool halo_point(int lt, int q, int& bi, int& bj, int&
     bj = lt & 7;
     bk = lt < 32 ? -1 : 32;
     return true;
+}
+
+// global cell of face-neighbour point u of thread lt around tile ti, or -1 (no point, or outside the domain)
+__device__ __forceinline__ int halo_cell(const TileItem& ti, int n, int lt, int u) {
+    int bi = 0, bj = 0, bk = 0;
+    if (!halo_point(lt, u, bi, bj, bk)) return -1;
+    const int gi = ti.i0 + bi, gj = ti.j0 + bj, gk = ti.k0 + bk;
+    if (gi < 0 || gi >= n || gj < 0 || gj >= n || gk < 0 || gk >= n) return -1;
+    return (gi * n + gj) * n + gk;
+}
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 
 template <int MAXC>
@@ -1859,13 +1877,6 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     double* const bufB = ws.partB;
     const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
     float* xg = S.p;
-    float* const Dg = S.pdiag;
-    float* const R0 = S.cg_r;
-    float* const R1 = S.cg_z;
-    float* const A0 = S.cg_Ap;
-    float* const A1 = S.hdiag;
-    float* const P0 = S.cg_p[0];
-    float* const P1 = S.cg_p[1];
     TileItem my[MAXC];
     bool have[MAXC];
 #pragma unroll
@@ -1875,15 +1886,23 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         my[q] = tiles[have[q] ? c : c0];
     }
     auto slot_of = [&](int q) { return sm_slots + (size_t)(g * MAXC + q) * kOneSlotFloats; };
+    unsigned phase_bit = 0;
+    auto wait_boxes = [&]() {
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], phase_bit) && ok;
+        if (!ok) atomicExch(ws.err, 1);
+        phase_bit ^= 1u;
+    };
     if (lt == 0) {
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) mbar_init(&mbar[g * MAXC + q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    float r[CPT], pv[CPT];
+    float r[CPT], ap[CPT], dg[CPT];
     int k = 0;
-    bool faces_requested = false;
     // ------------------------------------------------------------------------------------------ set-up
     float mean = 0.0f;
     {
@@ -1893,28 +1912,26 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         mean = __double2float_rn(mm[0] / ((double)n * n * n));
     }
     {
-        // r0 = b - A x0, z0 = D r0, p0 = z0 (published for the halo of A p0); partials b.b, r.r, r.z
+        // r0 = b - A x0, p0 = z0 = D r0 (published for the halo of A p0); partials b.b, r.r, r.z
         __syncthreads();   // red is free (the rhs mean above read it)
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) {
             double part[3] = {0.0, 0.0, 0.0};
-            float* cells = slot_of(q) + kOneCells;
+            float* X = slot_of(q) + kOneCells;
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
                 const int s = q * 4 + m, e = m * 256 + lt;
-                r[s] = pv[s] = 0.0f;
-                cells[e] = cells[1024 + e] = cells[2048 + e] = 0.0f;
+                r[s] = ap[s] = dg[s] = 0.0f;
+                X[e] = 0.0f;
                 const Cell cl = tile_cell(my[q], n, lt, m);
                 if (!have[q] || !cl.ok) continue;
                 float b, d, rr;
                 setup_cell<false>(S, xg, mean, hh, 0.0f, cl, b, d, rr);
                 const float z = __fmul_rn(d, rr);
-                cells[e] = xg[cl.t];
-                cells[1024 + e] = d;
-                Dg[cl.t] = d;
+                X[e] = xg[cl.t];
+                dg[s] = d;
                 r[s] = rr;
-                pv[s] = z;
-                P0[cl.t] = z;
+                S.cg_p[0][cl.t] = z;
                 part[0] += (double)b * (double)b;
                 part[1] += (double)rr * (double)rr;
                 part[2] += (double)rr * (double)z;
@@ -1936,15 +1953,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             tma_load_3d(slot + kOneFaces + kBX + kBY, &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
         }
     }
-    faces_requested = true;
-    {
-        bool ok = true;
-#pragma unroll
-        for (int q = 0; q < MAXC; ++q)
-            if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], 0) && ok;
-        if (!ok) atomicExch(ws.err, 1);
-    }
-    faces_requested = false;
+    wait_boxes();
     if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
     {
         double tot[3];
@@ -1960,10 +1969,38 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     // ------------------------------------------------------------------------------------------ iterations
     // k = 0 forms A p0 from the published p0; k >= 1 first advances x, r and p with the scalars of iteration k - 1
     for (k = 0;; ++k) {
-        const int cur = k & 1, prev = cur ^ 1;
+        const int prev = (k & 1) ^ 1;
+        // p_{k-1} boxes (TMA) and the neighbours' z', q (cp.async), requested before the scene sums
+        if (lt == 0) {
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                if (!have[q]) continue;
+                unsigned long long* mb = &mbar[g * MAXC + q];
+                mbar_expect_tx(mb, (unsigned)(kBZ * sizeof(float)));
+                // k = 0: p0 in buffer 0; k >= 1: p_{k-1} in buffer (k - 1) & 1
+                tma_load_3d(slot_of(q), (k == 0 || prev == 0) ? &maps.p0 : &maps.p1, my[q].k0 - 4, my[q].j0 - 1,
+                            my[q].i0 - 1, mb);
+            }
+        }
+        if (k > 0) {
+            const float* Zp = prev ? S.cg_z : S.cg_r;
+            const float* Qp = prev ? S.hdiag : S.cg_Ap;
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                float* stg = slot_of(q) + kOneHalo;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int t = have[q] ? halo_cell(my[q], n, lt, u) : -1;
+                    if (t < 0) continue;
+                    cp_async4(stg + u * 256 + lt, Zp + t);
+                    cp_async4(stg + kOneHaloPts + u * 256 + lt, Qp + t);
+                }
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        }
         float alpha = 0.0f, beta = 0.0f;
-        // the halo of p_k: the neighbours' published values, loaded right after the barrier
-        float hr[4], ha[4], hp[4], hd[4];
         if (k > 0) {
             double tot[kOneComps];
             // pAp, rr, rz, Ap.z, Ap.D.Ap of iteration k - 1
@@ -1993,103 +2030,75 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 }
             }
             __syncthreads();
-            if (!Ls.live) break;
             alpha = Ls.alpha;
             beta = Ls.beta;
         }
-        // p_k in every tile's box: own cells from registers, face neighbours recomputed from their published values
-        {
-            const float* Rp = prev ? R1 : R0;
-            const float* Ap_ = prev ? A1 : A0;
-            const float* Pp = prev ? P1 : P0;
+        wait_boxes();
+        if (k > 0) asm volatile("cp.async.wait_all;" ::: "memory");
+        asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory");
+        if (!Ls.live) break;
+        if (k > 0) {
+            // p_k everywhere in the boxes by one formula: z = z' - alpha q, p = z + beta p_{k-1}; own cells also
+            // advance x and r
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
                 float* box = slot_of(q);
-                int ho[4];
+                const float* stg = box + kOneHalo;
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     int bi = 0, bj = 0, bk = 0;
-                    ho[u] = -1;
-                    if (!have[q] || !halo_point(lt, u, bi, bj, bk)) continue;
-                    const int gi = my[q].i0 + bi, gj = my[q].j0 + bj, gk = my[q].k0 + bk;
-                    if (gi < 0 || gi >= n || gj < 0 || gj >= n || gk < 0 || gk >= n) continue;
-                    ho[u] = (gi * n + gj) * n + gk;
-                }
-                // k = 0: p0 itself (published in the set-up, buffer 0); k >= 1: D (r - alpha Ap) + beta p
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int t = ho[u];
-                    if (t < 0) continue;
-                    if (k == 0) {
-                        hp[u] = P0[t];
-                    } else {
-                        hr[u] = Rp[t];
-                        ha[u] = Ap_[t];
-                        hp[u] = Pp[t];
-                        hd[u] = Dg[t];
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int t = ho[u];
-                    if (t < 0) continue;
-                    int bi = 0, bj = 0, bk = 0;
+                    if (!have[q] || halo_cell(my[q], n, lt, u) < 0) continue;
                     halo_point(lt, u, bi, bj, bk);
-                    float pk = hp[u];
-                    if (k > 0)
-                        pk = __fadd_rn(__fmul_rn(hd[u], __fsub_rn(hr[u], __fmul_rn(alpha, ha[u]))), __fmul_rn(beta, pk));
-                    box[(bi + 1) * 400 + (bj + 1) * 40 + (bk + 4)] = pk;
+                    float& pb = box[(bi + 1) * 400 + (bj + 1) * 40 + (bk + 4)];
+                    const float z = __fsub_rn(stg[u * 256 + lt], __fmul_rn(alpha, stg[kOneHaloPts + u * 256 + lt]));
+                    pb = __fadd_rn(z, __fmul_rn(beta, pb));
                 }
-                float* X = slot_of(q) + kOneCells;
-                const float* Dc = X + 1024;
-                const float* Apc = X + 2048;
+                float* X = box + kOneCells;
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
                     const int s = q * 4 + m, e = m * 256 + lt;
                     const Cell cl = tile_cell(my[q], n, lt, m);
                     if (!have[q] || !cl.ok) continue;
-                    if (k > 0) {
-                        // x_k = x_{k-1} + alpha p_{k-1}; r_k = r_{k-1} - alpha A p_{k-1}; p_k = D r_k + beta p_{k-1}
-                        X[e] = __fadd_rn(X[e], __fmul_rn(alpha, pv[s]));
-                        r[s] = __fsub_rn(r[s], __fmul_rn(alpha, Apc[e]));
-                        pv[s] = __fadd_rn(__fmul_rn(Dc[e], r[s]), __fmul_rn(beta, pv[s]));
-                    }
-                    box[(m + 1) * 400 + ((lt >> 5) + 1) * 40 + ((lt & 31) + 4)] = pv[s];
+                    float& pb = box[(m + 1) * 400 + ((lt >> 5) + 1) * 40 + ((lt & 31) + 4)];
+                    const float zp = __fmul_rn(dg[s], r[s]), qv = __fmul_rn(dg[s], ap[s]);
+                    const float z = __fsub_rn(zp, __fmul_rn(alpha, qv));
+                    X[e] = __fadd_rn(X[e], __fmul_rn(alpha, pb));
+                    r[s] = __fsub_rn(r[s], __fmul_rn(alpha, ap[s]));
+                    pb = __fadd_rn(z, __fmul_rn(beta, pb));
                 }
             }
+            asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory");
         }
-        asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory");
-        // A p_k from the box; partials of iteration k; publish r_k, A p_k, p_k for the neighbours' next halo
+        // A p_k from the box; partials of iteration k; publish p_k, z_k' = D r_k and q_k = D A p_k
         {
-            float* const Rc = cur ? R1 : R0;
-            float* const Ac = cur ? A1 : A0;
-            float* const Pc = cur ? P1 : P0;
+            const int cur = k & 1;
+            float* const Zc = cur ? S.cg_z : S.cg_r;
+            float* const Qc = cur ? S.hdiag : S.cg_Ap;
+            float* const Pc = cur ? S.cg_p[1] : S.cg_p[0];
             __syncthreads();   // red is free (the scene sums above read it)
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
                 double part[kOneComps] = {0.0, 0.0, 0.0, 0.0, 0.0};
                 const float* slot = slot_of(q);
-                const float* Dc = slot + kOneCells + 1024;
-                float* Apc = slot_of(q) + kOneCells + 2048;
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
-                    const int s = q * 4 + m, e = m * 256 + lt;
+                    const int s = q * 4 + m;
                     const Cell cl = tile_cell(my[q], n, lt, m);
                     if (!have[q] || !cl.ok) continue;
                     const int bj = lt >> 5, bk = lt & 31, o = (m + 1) * 400 + (bj + 1) * 40 + (bk + 4);
-                    const float apv = lap_box(slot, slot + kOneFaces, slot + kOneFaces + kBX, slot + kOneFaces + kBX + kBY,
-                                              cl, n, m, bj, bk, o, hhd);
-                    Apc[e] = apv;
-                    const double d = Dc[e], a = apv, rs = r[s];
-                    const double z = __fmul_rn(Dc[e], r[s]);
-                    part[0] += (double)pv[s] * a;
+                    const float pk = slot[o];
+                    ap[s] = lap_box(slot, slot + kOneFaces, slot + kOneFaces + kBX, slot + kOneFaces + kBX + kBY, cl, n,
+                                    m, bj, bk, o, hhd);
+                    const float zp = __fmul_rn(dg[s], r[s]);
+                    const double d = dg[s], a = ap[s], rs = r[s], z = zp;
+                    part[0] += (double)pk * a;
                     part[1] += rs * rs;
                     part[2] += rs * z;
                     part[3] += a * z;
                     part[4] += a * (d * a);
-                    Rc[cl.t] = r[s];
-                    Ac[cl.t] = apv;
-                    Pc[cl.t] = pv[s];
+                    Zc[cl.t] = zp;
+                    Qc[cl.t] = __fmul_rn(dg[s], ap[s]);
+                    if (k > 0) Pc[cl.t] = pk;
                 }
                 stash_warp<kOneComps>(part, red, kOneComps * q);
             }
@@ -2123,12 +2132,13 @@ writeback:
         }
     }
 finish:
-    if (*(volatile int*)ws.err || faces_requested) {
-        // leave no copy in flight: the face boxes are waited for again (bounded) before the block exits
+    if (*(volatile int*)ws.err) {
+        // leave no copy in flight: the last requested boxes are waited for again (bounded) before the block exits
 #pragma unroll
         for (int q = 0; q < MAXC; ++q)
-            if (have[q]) mbar_wait(&mbar[g * MAXC + q], 0);
+            if (have[q]) mbar_wait(&mbar[g * MAXC + q], phase_bit ^ 1u);
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     if (blockIdx.x == 0 && threadIdx.x == 0) write_stats(S, Ls, false, *(volatile int*)ws.err != 0, par);
 }
 
