@@ -239,7 +239,12 @@ int launch_resident(const hf_plan* p, DeviceInfo* d, bool heat, double dt, int s
     // staged and its scratch vectors exist
     const bool pipe = !heat && tma && (p->options & HF_PLAN_SINGLE_REDUCTION_CG) && sc.cg_r && sc.cg_z && sc.cg_Ap &&
                       sc.hdiag && sc.pdiag && sc.cg_p[0] && sc.cg_p[1];
-    for (int m = want ? want : 1; m <= 3; ++m) {
+    // tiles per group: the fewest that fit; the single-reduction pressure kernel prefers three (two 256-thread groups
+    // of 128 registers per thread: its per-thread state does not fit the 80 registers of a 768-thread block)
+    const bool three_first = pipe && !want && tpb > 4;
+    for (int mi = 0; mi < 3; ++mi) {
+        const int m = want ? want + mi : (three_first ? 3 - mi : 1 + mi);
+        if (m > 3) break;
         const int groups = (tpb + m - 1) / m;
         if (groups > kResGroupsMax[m]) continue;
         const void* fn = pipe ? hf::pcg_one_kernel(m) : hf::pcg_resident_kernel(heat, m, tma);
