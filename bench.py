@@ -74,7 +74,7 @@ def parse():
                     help="plain: CG solves in the streaming kernel instead of the resident one")
     ap.add_argument("--persistent-blocks", type=int, default=0, help="plain: grid of the streaming CG kernel")
     ap.add_argument("--no-tma", action="store_true", help="plain: resident pressure CG without the TMA-staged stencil")
-    ap.add_argument("--cg", default="classic", choices=["classic", "single-reduction"],
+    ap.add_argument("--cg", default="single-reduction", choices=["classic", "single-reduction"],
                     help="plain: pressure solve by the classic Jacobi-PCG or its single-reduction form (one grid "
                          "barrier per iteration)")
     ap.add_argument("--scenes", type=int, default=64, help="batched: scenes in the ensemble")
@@ -445,14 +445,17 @@ def bench_plain(args, dev, rank, world, local):
     peaks = load_peaks()
     cg_bytes = pressure_bytes_per_launch(N, p_iters / steps)
     traffic = None
+    single = args.cg == "single-reduction"
     try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "pressure_cg_96.json")))
+        prof = json.load(open(os.path.join(ROOT, "profiles", "pressure_cg_one_96.json" if single else "pressure_cg_96.json")))
         traffic = prof["dram_bytes_per_iteration"] * (p_iters / steps) + prof.get("dram_bytes_fixed", 0.0)
     except (OSError, ValueError, KeyError):
         pass
-    roof = roofline(cg_bytes / (cg_ms / steps / 1000.0) / 1e9, peaks, traffic=traffic,
-                    kernel="k_pcg_tma<2> (pressure Jacobi-PCG + projection, one persistent cooperative launch, "
-                           "TMA-staged register-resident stencil)",
+    kernel = ("k_pcg_one<3> (single-reduction pressure Jacobi-PCG + projection: one grid barrier per iteration, one "
+              "persistent cooperative launch, TMA-staged register-resident stencil)" if single else
+              "k_pcg_tma<2> (pressure Jacobi-PCG + projection, one persistent cooperative launch, TMA-staged "
+              "register-resident stencil)")
+    roof = roofline(cg_bytes / (cg_ms / steps / 1000.0) / 1e9, peaks, traffic=traffic, kernel=kernel,
                     bytes_per_launch=cg_bytes, ms_per_launch=cg_ms / steps, mean_pressure_iters=p_iters / steps)
     sb = substep_bytes(N, h_iters / steps, p_iters / steps, True)
     sub_gbs = sb / (el_ms / steps / 1000.0) / 1e9
@@ -491,7 +494,8 @@ def bench_plain(args, dev, rank, world, local):
                         "mean_pressure_iters": p_iters / steps, "mean_heat_iters": h_iters / steps,
                         "cell_updates_per_s": value * N, "substep_status": int(st1.status),
                         "substep_roofline": sub_roof, "stage_ms": stage_ms,
-                        "timed_launches": "one CUDA-graph replay of the K substeps" if use_graph else "eager launches"},
+                        "timed_launches": "one CUDA-graph replay of the K substeps" if use_graph else "eager launches",
+                        "pressure_cg": args.cg},
             "parity": parity,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * steps, "clocks": ck}
 
