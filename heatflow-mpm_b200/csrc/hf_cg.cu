@@ -1483,6 +1483,25 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         my[q] = tiles[have[q] ? c : c0];
     }
     unsigned phase_bit = 0;
+    // the z and p_{k-1} boxes of iteration kit, requested by thread lt == 0 of each group; the next iteration's are
+    // requested right after the barrier that ends phase B, before the scene sums, so the copy overlaps them
+    auto issue_boxes = [&](int kit) {
+        if (lt != 0) return;
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q) {
+            if (!have[q]) continue;
+            float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
+            unsigned long long* mb = &mbar[g * MAXC + q];
+            mbar_expect_tx(mb, (unsigned)((kit == 1 ? 1 : 2) * kBZ * sizeof(float)));
+            tma_load_3d(slot, &maps.z, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
+            if (kit != 1)
+                tma_load_3d(slot + kBZ, ((kit - 1) & 1) ? &maps.p1 : &maps.p0, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1,
+                            mb);
+        }
+    };
+    bool requested = false;   // the next iteration's boxes are in flight
     if (lt == 0) {
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) mbar_init(&mbar[g * MAXC + q], 1);
@@ -1557,6 +1576,8 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         phase_bit ^= 1u;
     }
     if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
+    issue_boxes(1);
+    requested = true;
     {
         double tot[3];
         const int comp[3] = {0, 1, 2};
@@ -1572,22 +1593,10 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         const float beta = Ls.beta;
         const bool first = kit == 1;
         float* pnew = S.cg_p[kit & 1];
-        // phase A: stage z and p_{k-1} with halo, form p_k in place, Ap from shared memory
-        if (lt == 0) {
-            asm volatile("fence.proxy.async.global;" ::: "memory");
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-#pragma unroll
-            for (int q = 0; q < MAXC; ++q) {
-                if (!have[q]) continue;
-                float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
-                unsigned long long* mb = &mbar[g * MAXC + q];
-                mbar_expect_tx(mb, (unsigned)((first ? 1 : 2) * kBZ * sizeof(float)));
-                tma_load_3d(slot, &maps.z, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
-                if (!first)
-                    tma_load_3d(slot + kBZ, ((kit - 1) & 1) ? &maps.p1 : &maps.p0, my[q].k0 - 4, my[q].j0 - 1,
-                                my[q].i0 - 1, mb);
-            }
-        }
+        // phase A: stage z and p_{k-1} with halo (requested after the previous barrier), form p_k in place, Ap from
+        // shared memory
+        if (!requested) issue_boxes(kit);
+        requested = false;
         {
             bool ok = true;
 #pragma unroll
@@ -1729,6 +1738,8 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             }
         }
         if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
+        issue_boxes(kit + 1);
+        requested = true;
         {
             double tot[2];
             const int comp[2] = {1, 2};
@@ -1736,6 +1747,16 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             if (threadIdx.x == 0) update_scalars(Ls, HEAT, tot[0], tot[1], kit);
             __syncthreads();
         }
+    }
+    if (requested) {
+        // the solve ended: the boxes requested for an iteration that does not run are waited for (no copy in flight)
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], phase_bit) && ok;
+        if (!ok) atomicExch(ws.err, 1);
+        phase_bit ^= 1u;
+        requested = false;
     }
     // -------------------------------------------------- write x back, then (pressure) project the faces
 #pragma unroll
