@@ -162,24 +162,25 @@ __device__ __forceinline__ void scene_sums_wide(const double* __restrict__ buf, 
     }
 }
 
-// scene_sums for K components on G >= 3 groups of 256 threads (blockDim >= 768): group q sums components q, q + 3, ...
-// each exactly as scene_sums' first 256 threads do (the same tree, the same bits), with ceil(K / 3) of them per thread.
-template <int K, int STRIDE>
+// scene_sums for K components spread over G groups of 256 threads (blockDim >= 256 G): group q sums components q,
+// q + G, q + 2 G, ... each exactly as scene_sums' first 256 threads do (the same tree, the same bits), with ceil(K / G)
+// of them per thread.
+template <int K, int STRIDE, int G = 3>
 __device__ __forceinline__ void scene_sums_3g(const double* __restrict__ buf, int b, int e, double (&tot)[K],
                                               double* red) {
-    constexpr int KPT = (K + 2) / 3;
+    constexpr int KPT = (K + G - 1) / G;
     const int q = threadIdx.x >> 8, lt = threadIdx.x & 255;
     double acc[KPT];
 #pragma unroll
     for (int j = 0; j < KPT; ++j) acc[j] = 0.0;
-    if (q < 3) {
+    if (q < G) {
         int c = b + lt;
         for (; c + 3 * kThreads < e; c += 4 * kThreads) {
             double v[KPT][4];
 #pragma unroll
             for (int j = 0; j < KPT; ++j)
 #pragma unroll
-                for (int u = 0; u < 4; ++u) v[j][u] = q + 3 * j < K ? buf[STRIDE * (c + u * kThreads) + q + 3 * j] : 0.0;
+                for (int u = 0; u < 4; ++u) v[j][u] = q + G * j < K ? buf[STRIDE * (c + u * kThreads) + q + G * j] : 0.0;
 #pragma unroll
             for (int j = 0; j < KPT; ++j)
 #pragma unroll
@@ -188,7 +189,7 @@ __device__ __forceinline__ void scene_sums_3g(const double* __restrict__ buf, in
         for (; c < e; c += kThreads) {
 #pragma unroll
             for (int j = 0; j < KPT; ++j)
-                if (q + 3 * j < K) acc[j] += buf[STRIDE * c + q + 3 * j];
+                if (q + G * j < K) acc[j] += buf[STRIDE * c + q + G * j];
         }
 #pragma unroll
         for (int j = 0; j < KPT; ++j) {
@@ -198,10 +199,10 @@ __device__ __forceinline__ void scene_sums_3g(const double* __restrict__ buf, in
     }
     const int lane = threadIdx.x & 31, wq = lt >> 5;
     __syncthreads();
-    if (q < 3 && lane == 0) {
+    if (q < G && lane == 0) {
 #pragma unroll
         for (int j = 0; j < KPT; ++j)
-            if (q + 3 * j < K) red[(q + 3 * j) * 32 + wq] = acc[j];
+            if (q + G * j < K) red[(q + G * j) * 32 + wq] = acc[j];
     }
     __syncthreads();
 #pragma unroll
@@ -2026,7 +2027,9 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             double tot[kOneComps];
             // pAp, rr, rz, Ap.z, Ap.D.Ap of iteration k - 1
             if (MAXC < 3 && blockDim.x >= 3 * kThreads) {
-                scene_sums_3g<kOneComps, kOneComps>(prev ? bufB : bufA, cb, ce, tot, red);
+                scene_sums_3g<kOneComps, kOneComps, 3>(prev ? bufB : bufA, cb, ce, tot, red);
+            } else if (blockDim.x >= 2 * kThreads) {
+                scene_sums_3g<kOneComps, kOneComps, 2>(prev ? bufB : bufA, cb, ce, tot, red);
             } else {
                 const int comp[kOneComps] = {0, 1, 2, 3, 4};
                 scene_sums<kOneComps, kOneComps>(prev ? bufB : bufA, cb, ce, comp, tot, red);
