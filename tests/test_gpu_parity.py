@@ -353,3 +353,35 @@ def test_sampling_stages_bit_exact_vs_oracle(torch_cuda):
            uvw[2], T2)
     got = sc.T[par ^ 1].cpu().numpy()
     assert np.array_equal(got.view(np.int32), T2.view(np.int32)), int((got != T2).sum())
+
+
+@pytest.mark.parametrize("n", [36, 44, 92])
+def test_single_reduction_partial_tiles_vs_oracle(torch_cuda, n):
+    """The single-reduction pressure solve on edges whose tiles are cut by the domain (n % 8 != 0, n % 32 != 0: partial
+    tiles in j and k, face-neighbour points outside the domain; 92: three tiles per group), tolerance 1e-6, 3 substeps:
+    GPU vs oracle, relative L2 <= 1e-5, every solve converged, iteration counts within 2 of the classic method's."""
+    import os
+    from heatflow_mpm.scene import DeviceScene, ScenePlan
+    from oracle import oracle as O
+    O.set_threads(len(os.sched_getaffinity(0)))
+    spec, T0, uvw = random_scene_inputs(n, seed=40 + n)
+    spec.cg_tol = 1e-6
+    sc = DeviceScene(spec)
+    for nm, a in zip("uvw", uvw):
+        sc.set_current(nm, a)
+    sc.set_current("T", T0)
+    plan = ScenePlan([sc])
+    plan.single_reduction_cg = True
+    plan.prepare_statics()
+    orc = oracle_from_spec(spec)
+    orc.set_state(T=T0, u=uvw[0], v=uvw[1], w=uvw[2])
+    for s in range(3):
+        plan.substep(2e-3)
+        orc.substep(2e-3)
+        st, ost = sc.read_state(), orc.stats()
+        assert st.status == 0, (s, st.status)
+        assert st.pressure_rr <= st.pressure_atol ** 2 * (1 + 1e-12)
+        assert abs(st.pressure_iters - ost["grid_done"]) <= 2, (s, st.pressure_iters, ost["grid_done"])
+        for nm in ("T", "u", "v", "w"):
+            got = sc.current(nm).cpu().numpy()
+            assert rel_l2(got, getattr(orc, nm)) <= 1e-5, (nm, s, rel_l2(got, getattr(orc, nm)))
