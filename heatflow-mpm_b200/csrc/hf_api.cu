@@ -247,6 +247,8 @@ int launch_resident(const hf_plan* p, DeviceInfo* d, bool heat, double dt, int s
         if (m > 3) break;
         const int groups = (tpb + m - 1) / m;
         if (groups > kResGroupsMax[m]) continue;
+        // the single-reduction kernel publishes one set of partials per 256-thread group into buffers sized by tiles
+        if (pipe && G * groups > nt) continue;
         const void* fn = pipe ? hf::pcg_one_kernel(m) : hf::pcg_resident_kernel(heat, m, tma);
         const size_t smem = pipe ? hf::pcg_one_smem(groups, m) : hf::pcg_resident_smem(groups, m, tma, heat);
         if (smem > d->smem_optin) continue;

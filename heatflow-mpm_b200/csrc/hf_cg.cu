@@ -79,30 +79,26 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& epoch, int
 // Sum of a scene's partials (item c, component comp[q] at buf[STRIDE * c + comp[q]]) in a fixed tree: the first 256
 // threads stride over the items in order, warp butterfly, then 8 warps in order.  Every block computing it obtains the
 // same bits.  STRIDE is 3 for the tile partials and 1 for the per-chunk rhs sums.
-template <int K, int STRIDE = 3>
+template <int K, int STRIDE = 3, int U = 4>
 __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b, int e, const int (&comp)[K],
                                            double (&tot)[K], double* red) {
     static_assert(K <= kRedComps, "red holds kRedComps components");
 #pragma unroll
     for (int q = 0; q < K; ++q) tot[q] = 0.0;
     if (threadIdx.x < kThreads) {
-        // a thread's partials c = b + t, b + t + 256, ... are added in that order; four are loaded before they are
-        // added, so their L2 round trips overlap instead of each waiting for the previous addition
-        int c = b + threadIdx.x;
-        for (; c + 3 * kThreads < e; c += 4 * kThreads) {
-            double v[4][K];
+        // a thread's partials c = b + t, b + t + 256, ... are added in that order; U at a time are loaded (an absent
+        // one as +0.0, which leaves a sum that started at +0.0 unchanged) before they are added, so their L2 round
+        // trips overlap instead of each waiting for the previous addition
+        for (int c = b + threadIdx.x; c < e; c += U * kThreads) {
+            double v[U][K];
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < U; ++u)
 #pragma unroll
-                for (int q = 0; q < K; ++q) v[u][q] = buf[STRIDE * (c + u * kThreads) + comp[q]];
+                for (int q = 0; q < K; ++q) v[u][q] = c + u * kThreads < e ? buf[STRIDE * (c + u * kThreads) + comp[q]] : 0.0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int q = 0; q < K; ++q) tot[q] += v[u][q];
-        }
-        for (; c < e; c += kThreads) {
-#pragma unroll
-            for (int q = 0; q < K; ++q) tot[q] += buf[STRIDE * c + comp[q]];
         }
     }
 #pragma unroll
@@ -137,15 +133,13 @@ __device__ __forceinline__ void scene_sums_wide(const double* __restrict__ buf, 
     double acc = 0.0;
     if (q < K) {
         const int cq = comp0 + q;
-        int c = b + lt;
-        for (; c + 3 * kThreads < e; c += 4 * kThreads) {
+        for (int c = b + lt; c < e; c += 4 * kThreads) {
             double v[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = buf[STRIDE * (c + u * kThreads) + cq];
+            for (int u = 0; u < 4; ++u) v[u] = c + u * kThreads < e ? buf[STRIDE * (c + u * kThreads) + cq] : 0.0;
 #pragma unroll
             for (int u = 0; u < 4; ++u) acc += v[u];
         }
-        for (; c < e; c += kThreads) acc += buf[STRIDE * c + cq];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     }
@@ -164,8 +158,8 @@ __device__ __forceinline__ void scene_sums_wide(const double* __restrict__ buf, 
 
 // scene_sums for K components spread over G groups of 256 threads (blockDim >= 256 G): group q sums components q,
 // q + G, q + 2 G, ... each exactly as scene_sums' first 256 threads do (the same tree, the same bits), with ceil(K / G)
-// of them per thread.
-template <int K, int STRIDE, int G = 3>
+// of them per thread, U partials of each loaded at a time.
+template <int K, int STRIDE, int G = 3, int U = 4>
 __device__ __forceinline__ void scene_sums_3g(const double* __restrict__ buf, int b, int e, double (&tot)[K],
                                               double* red) {
     constexpr int KPT = (K + G - 1) / G;
@@ -174,22 +168,17 @@ __device__ __forceinline__ void scene_sums_3g(const double* __restrict__ buf, in
 #pragma unroll
     for (int j = 0; j < KPT; ++j) acc[j] = 0.0;
     if (q < G) {
-        int c = b + lt;
-        for (; c + 3 * kThreads < e; c += 4 * kThreads) {
-            double v[KPT][4];
+        for (int c = b + lt; c < e; c += U * kThreads) {
+            double v[KPT][U];
 #pragma unroll
             for (int j = 0; j < KPT; ++j)
 #pragma unroll
-                for (int u = 0; u < 4; ++u) v[j][u] = q + G * j < K ? buf[STRIDE * (c + u * kThreads) + q + G * j] : 0.0;
+                for (int u = 0; u < U; ++u)
+                    v[j][u] = q + G * j < K && c + u * kThreads < e ? buf[STRIDE * (c + u * kThreads) + q + G * j] : 0.0;
 #pragma unroll
             for (int j = 0; j < KPT; ++j)
 #pragma unroll
-                for (int u = 0; u < 4; ++u) acc[j] += v[j][u];
-        }
-        for (; c < e; c += kThreads) {
-#pragma unroll
-            for (int j = 0; j < KPT; ++j)
-                if (q + G * j < K) acc[j] += buf[STRIDE * c + q + G * j];
+                for (int u = 0; u < U; ++u) acc[j] += v[j][u];
         }
 #pragma unroll
         for (int j = 0; j < KPT; ++j) {
@@ -279,24 +268,19 @@ __device__ __forceinline__ void publish_group(const double* red, double* __restr
     }
 }
 
-// publish_group for K components per tile at stride K (the single-reduction CG's five partials)
-template <int MAXC, int K>
-__device__ __forceinline__ void publish_k(const double* red, double* __restrict__ buf, int first_tile, int groups,
-                                          int c_end) {
+// One partial per 256-thread group (the single-reduction CG's five components, stride K): after stash_warp<K>(v, red,
+// 0) in every warp, thread lt == 0 of each group adds its 8 warps in order and writes buf[K * unit + comp].
+template <int K>
+__device__ __forceinline__ void publish_unit(const double* red, double* __restrict__ buf, int unit) {
     __syncthreads();
     if ((threadIdx.x & 255) == 0) {
         const int g0 = (threadIdx.x >> 5);
 #pragma unroll
-        for (int q = 0; q < MAXC; ++q) {
-            const int c = first_tile + groups * q;
-            if (c >= c_end) continue;
+        for (int comp = 0; comp < K; ++comp) {
+            double s = 0.0;
 #pragma unroll
-            for (int comp = 0; comp < K; ++comp) {
-                double s = 0.0;
-#pragma unroll
-                for (int w = 0; w < 8; ++w) s += red[(K * q + comp) * 32 + g0 + w];
-                buf[K * c + comp] = s;
-            }
+            for (int w = 0; w < 8; ++w) s += red[comp * 32 + g0 + w];
+            buf[K * unit + comp] = s;
         }
     }
 }
@@ -1806,6 +1790,11 @@ finish:
 // 1e-6 too).  The convergence test is the classic one on the direct r_k . r_k, taken at the barrier after r_k was
 // formed: a solve stops with the same x and reports the same iteration count.
 //
+// Partials: a thread adds the five products of its cells in cell order, the warp butterfly and the group's 8 warps in
+// order give one set per 256-thread group, and every block sums the groups' sets in group order (the set-up's three
+// sums stay per tile).  The tree is fixed for a given grid, so a solve is deterministic; unlike the classic variants'
+// per-tile tree it depends on the launch shape (this kernel only runs single-scene plans).
+//
 // Halo: iteration k + 1 needs p_{k+1} = z_{k+1} + beta p_k at the tile's face neighbours, which belong to other
 // blocks.  Every block publishes, for its cells, p_k, z_k' = D r_k and q_k = D A p_k (double-buffered: p in cg_p[0] /
 // cg_p[1], z' in cg_r / cg_z, q in cg_Ap / hdiag -- the heat diagonal is dead while the pressure system is solved).
@@ -1819,7 +1808,7 @@ constexpr int kOneCells = kBZ + kBX + kBY + kBW;          // slot offset of x (1
 constexpr int kOneHalo = kOneCells + 1024;                // slot offset of the halo staging: z' and q of 832 points
 constexpr int kOneHaloPts = 832;
 constexpr int kOneSlotFloats = kOneHalo + 2 * kOneHaloPts;   // 8672 floats = 34,688 bytes (a multiple of 128)
-constexpr int kOneComps = 5;                              // partials per tile: pAp, rr, rz, Ap.z, Ap.D.Ap
+constexpr int kOneComps = 5;                              // partials per group: pAp, rr, rz, Ap.z, Ap.D.Ap
 static_assert(kOneSlotFloats % 32 == 0, "slots stay 128-byte aligned");
 
 // grid.py:94-115 k_laplacian of one tile cell from a staged box (centre offset o) and the tile's face boxes
@@ -1881,7 +1870,9 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     constexpr int CPT = 4 * MAXC;
     extern __shared__ __align__(128) float sm_raw[];
     float* sm_slots = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
-    __shared__ double red[kOneComps * 3 * 32];   // five partials of up to three tiles per group, one per warp
+    __shared__ double red[kOneComps * 3 * 32];   // five partials per warp (the set-up: three of up to three tiles)
+    __shared__ unsigned hmask_s[1024];
+    __shared__ TileItem my_s[4 * 3];
     __shared__ LocalScene Ls;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
     const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
@@ -1898,14 +1889,19 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     double* const bufA = ws.partA;
     double* const bufB = ws.partB;
     const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
+    // the iterations' partials: one per 256-thread group, unit = block x groups + group (the launch keeps the units
+    // within the tile count that the partial buffers are sized for)
+    const int units = (int)gridDim.x * groups, unit = (int)blockIdx.x * groups + g;
     float* xg = S.p;
-    TileItem my[MAXC];
+    // the group's tiles (shared memory, like the halo mask below: registers held through the solve make the stencil
+    // phase spill)
+    TileItem* const my = my_s + g * MAXC;
     bool have[MAXC];
 #pragma unroll
-    for (int q = 0; q < MAXC; ++q) {
-        const int c = c0 + g + groups * q;
-        have[q] = c < c1;
-        my[q] = tiles[have[q] ? c : c0];
+    for (int q = 0; q < MAXC; ++q) have[q] = c0 + g + groups * q < c1;
+    if (lt < MAXC) {
+        const int c = c0 + g + groups * lt;
+        my[lt] = tiles[c < c1 ? c : c0];
     }
     auto slot_of = [&](int q) { return sm_slots + (size_t)(g * MAXC + q) * kOneSlotFloats; };
     unsigned phase_bit = 0;
@@ -1923,6 +1919,16 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    // bit 4 q + u of hmask_s[thread]: the thread's face-neighbour point u of tile q exists and lies in the domain
+    {
+        unsigned hm = 0;
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (have[q] && halo_cell(my[q], n, lt, u) >= 0) hm |= 1u << (4 * q + u);
+        hmask_s[threadIdx.x] = hm;
+    }
     float r[CPT], ap[CPT], dg[CPT];
     int k = 0;
     // ------------------------------------------------------------------------------------------ set-up
@@ -2009,13 +2015,17 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         if (k > 0) {
             const float* Zp = prev ? S.cg_z : S.cg_r;
             const float* Qp = prev ? S.hdiag : S.cg_Ap;
+            const unsigned hmask = hmask_s[threadIdx.x];
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
                 float* stg = slot_of(q) + kOneHalo;
+                const int tb = (my[q].i0 * n + my[q].j0) * n + my[q].k0;
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    const int t = have[q] ? halo_cell(my[q], n, lt, u) : -1;
-                    if (t < 0) continue;
+                    int bi = 0, bj = 0, bk = 0;
+                    if (!((hmask >> (4 * q + u)) & 1u)) continue;
+                    halo_point(lt, u, bi, bj, bk);
+                    const int t = tb + (bi * n + bj) * n + bk;
                     cp_async4(stg + u * 256 + lt, Zp + t);
                     cp_async4(stg + kOneHaloPts + u * 256 + lt, Qp + t);
                 }
@@ -2025,14 +2035,14 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         float alpha = 0.0f, beta = 0.0f;
         if (k > 0) {
             double tot[kOneComps];
-            // pAp, rr, rz, Ap.z, Ap.D.Ap of iteration k - 1
+            // pAp, rr, rz, Ap.z, Ap.D.Ap of iteration k - 1: the groups' partials in group order
             if (MAXC < 3 && blockDim.x >= 3 * kThreads) {
-                scene_sums_3g<kOneComps, kOneComps, 3>(prev ? bufB : bufA, cb, ce, tot, red);
+                scene_sums_3g<kOneComps, kOneComps, 3, 2>(prev ? bufB : bufA, 0, units, tot, red);
             } else if (blockDim.x >= 2 * kThreads) {
-                scene_sums_3g<kOneComps, kOneComps, 2>(prev ? bufB : bufA, cb, ce, tot, red);
+                scene_sums_3g<kOneComps, kOneComps, 2, 2>(prev ? bufB : bufA, 0, units, tot, red);
             } else {
                 const int comp[kOneComps] = {0, 1, 2, 3, 4};
-                scene_sums<kOneComps, kOneComps>(prev ? bufB : bufA, cb, ce, comp, tot, red);
+                scene_sums<kOneComps, kOneComps, 1>(prev ? bufB : bufA, 0, units, comp, tot, red);
             }
             if (threadIdx.x == 0) {
                 // the classic test on r_{k-1} (formed in iteration k - 1): converged -> x_{k-1} is the solution
@@ -2064,6 +2074,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         if (k > 0) {
             // p_k everywhere in the boxes by one formula: z = z' - alpha q, p = z + beta p_{k-1}; own cells also
             // advance x and r
+            const unsigned hmask = hmask_s[threadIdx.x];
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
                 float* box = slot_of(q);
@@ -2071,7 +2082,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     int bi = 0, bj = 0, bk = 0;
-                    if (!have[q] || halo_cell(my[q], n, lt, u) < 0) continue;
+                    if (!((hmask >> (4 * q + u)) & 1u)) continue;
                     halo_point(lt, u, bi, bj, bk);
                     float& pb = box[(bi + 1) * 400 + (bj + 1) * 40 + (bk + 4)];
                     const float z = __fsub_rn(stg[u * 256 + lt], __fmul_rn(alpha, stg[kOneHaloPts + u * 256 + lt]));
@@ -2100,9 +2111,10 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             float* const Qc = cur ? S.hdiag : S.cg_Ap;
             float* const Pc = cur ? S.cg_p[1] : S.cg_p[0];
             __syncthreads();   // red is free (the scene sums above read it)
+            // the five partials of the thread's cells, in cell order (tile q, then m)
+            double part[kOneComps] = {0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
-                double part[kOneComps] = {0.0, 0.0, 0.0, 0.0, 0.0};
                 const float* slot = slot_of(q);
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
@@ -2124,9 +2136,9 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                     Qc[cl.t] = __fmul_rn(dg[s], ap[s]);
                     if (k > 0) Pc[cl.t] = pk;
                 }
-                stash_warp<kOneComps>(part, red, kOneComps * q);
             }
-            publish_k<MAXC, kOneComps>(red, cur ? bufB : bufA, c0 + g, groups, c1);
+            stash_warp<kOneComps>(part, red, 0);
+            publish_unit<kOneComps>(red, cur ? bufB : bufA, unit);
         }
         if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
     }
