@@ -1145,6 +1145,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     __shared__ double red[kRedComps * 32];
     __shared__ LocalScene Ls;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
+    __shared__ TileItem my_s[4 * 3];
     const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
     const int c0 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * blockIdx.x) / gridDim.x);
     const int c1 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * (blockIdx.x + 1)) / gridDim.x);
@@ -1161,13 +1162,14 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
     float* xg = HEAT ? S.T[par ^ 1] : S.p;
     float* zg = S.cg_z;
-    TileItem my[MAXC];
+    // the group's tiles in shared memory (registers held through the solve make the stencil phases spill)
+    TileItem* const my = my_s + g * MAXC;
     bool have[MAXC];
 #pragma unroll
-    for (int q = 0; q < MAXC; ++q) {
-        const int c = c0 + g + groups * q;
-        have[q] = c < c1;
-        my[q] = tiles[have[q] ? c : c0];
+    for (int q = 0; q < MAXC; ++q) have[q] = c0 + g + groups * q < c1;
+    if (lt < MAXC) {
+        const int c = c0 + g + groups * lt;
+        my[lt] = tiles[c < c1 ? c : c0];
     }
     unsigned phase_bit = 0;
     if (TMA && lt == 0) {
@@ -1443,6 +1445,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     __shared__ double red[kRedComps * 32];
     __shared__ LocalScene Ls;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
+    __shared__ TileItem my_s[4 * 3];
     const int groups = blockDim.x >> 8, g = threadIdx.x >> 8, lt = threadIdx.x & 255;
     const int c0 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * blockIdx.x) / gridDim.x);
     const int c1 = tile_lo + (int)(((long long)(tile_hi - tile_lo) * (blockIdx.x + 1)) / gridDim.x);
@@ -1459,13 +1462,14 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     const int cb = ws.tile_begin[sidx], ce = ws.tile_begin[sidx + 1];
     float* xg = HEAT ? S.T[par ^ 1] : S.p;
     float* zg = S.cg_z;
-    TileItem my[MAXC];
+    // the group's tiles in shared memory (registers held through the solve make the stencil phases spill)
+    TileItem* const my = my_s + g * MAXC;
     bool have[MAXC];
 #pragma unroll
-    for (int q = 0; q < MAXC; ++q) {
-        const int c = c0 + g + groups * q;
-        have[q] = c < c1;
-        my[q] = tiles[have[q] ? c : c0];
+    for (int q = 0; q < MAXC; ++q) have[q] = c0 + g + groups * q < c1;
+    if (lt < MAXC) {
+        const int c = c0 + g + groups * lt;
+        my[lt] = tiles[c < c1 ? c : c0];
     }
     unsigned phase_bit = 0;
     // the z and p_{k-1} boxes of iteration kit, requested by thread lt == 0 of each group; the next iteration's are
@@ -1796,13 +1800,14 @@ finish:
 // per-tile tree it depends on the launch shape (this kernel only runs single-scene plans).
 //
 // Halo: iteration k + 1 needs p_{k+1} = z_{k+1} + beta p_k at the tile's face neighbours, which belong to other
-// blocks.  Every block publishes, for its cells, p_k, z_k' = D r_k and q_k = D A p_k (double-buffered: p in cg_p[0] /
-// cg_p[1], z' in cg_r / cg_z, q in cg_Ap / hdiag -- the heat diagonal is dead while the pressure system is solved).
-// Right after the barrier a block requests its tiles' p_k boxes (TMA) and the z', q values of their 832 face-neighbour
-// points (cp.async), both in flight while it sums the partials; then every p_{k+1} in its boxes, own cells and
-// neighbours alike, is formed by the same operations, z = z' - alpha q, p = z + beta p, so all blocks agree bit for
-// bit.  State: r, A p and D of a thread's cells in registers; x, the p box (one-cell halo), the face-fraction boxes
-// (TMA, once) and the halo staging in shared memory.
+// blocks.  Every block publishes, for the cells on its tiles' faces, z_k' = D r_k and q_k = D A p_k (double-buffered:
+// z' in cg_r / cg_z, q in cg_Ap / hdiag -- the heat diagonal is dead while the pressure system is solved).  Right
+// after the barrier a block requests the z', q values of its tiles' 832 face-neighbour points (cp.async), in flight
+// while it sums the partials; then every p_{k+1} in its boxes, own cells and neighbours alike, is formed by the same
+// operations from the same values, z = z' - alpha q, p = z + beta p, so all blocks agree bit for bit and no block
+// needs another's p: the p boxes (one-cell halo) are loaded once, from the published p0 (TMA), and advanced in place.
+// State: r, A p and D of a thread's cells in registers; x, the p box, the face-fraction boxes (TMA, once) and the
+// halo staging in shared memory.
 constexpr int kOneFaces = kBZ;                            // slot offset of the face-fraction boxes
 constexpr int kOneCells = kBZ + kBX + kBY + kBW;          // slot offset of x (1024 floats)
 constexpr int kOneHalo = kOneCells + 1024;                // slot offset of the halo staging: z' and q of 832 points
@@ -1998,8 +2003,9 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     // k = 0 forms A p0 from the published p0; k >= 1 first advances x, r and p with the scalars of iteration k - 1
     for (k = 0;; ++k) {
         const int prev = (k & 1) ^ 1;
-        // p_{k-1} boxes (TMA) and the neighbours' z', q (cp.async), requested before the scene sums
-        if (lt == 0) {
+        // k = 0: the p0 boxes (TMA), requested before the scene sums; after that the boxes stay in shared memory and
+        // every block advances its own copy of p at its tiles' cells and face neighbours
+        if (k == 0 && lt == 0) {
             asm volatile("fence.proxy.async.global;" ::: "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 #pragma unroll
@@ -2007,11 +2013,10 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 if (!have[q]) continue;
                 unsigned long long* mb = &mbar[g * MAXC + q];
                 mbar_expect_tx(mb, (unsigned)(kBZ * sizeof(float)));
-                // k = 0: p0 in buffer 0; k >= 1: p_{k-1} in buffer (k - 1) & 1
-                tma_load_3d(slot_of(q), (k == 0 || prev == 0) ? &maps.p0 : &maps.p1, my[q].k0 - 4, my[q].j0 - 1,
-                            my[q].i0 - 1, mb);
+                tma_load_3d(slot_of(q), &maps.p0, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
             }
         }
+        // k >= 1: the neighbours' z', q (cp.async), in flight during the scene sums
         if (k > 0) {
             const float* Zp = prev ? S.cg_z : S.cg_r;
             const float* Qp = prev ? S.hdiag : S.cg_Ap;
@@ -2067,7 +2072,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             alpha = Ls.alpha;
             beta = Ls.beta;
         }
-        wait_boxes();
+        if (k == 0) wait_boxes();
         if (k > 0) asm volatile("cp.async.wait_all;" ::: "memory");
         asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory");
         if (!Ls.live) break;
@@ -2104,12 +2109,11 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             }
             asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory");
         }
-        // A p_k from the box; partials of iteration k; publish p_k, z_k' = D r_k and q_k = D A p_k
+        // A p_k from the box; partials of iteration k; publish z_k' = D r_k and q_k = D A p_k
         {
             const int cur = k & 1;
             float* const Zc = cur ? S.cg_z : S.cg_r;
             float* const Qc = cur ? S.hdiag : S.cg_Ap;
-            float* const Pc = cur ? S.cg_p[1] : S.cg_p[0];
             __syncthreads();   // red is free (the scene sums above read it)
             // the five partials of the thread's cells, in cell order (tile q, then m)
             double part[kOneComps] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -2132,9 +2136,11 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                     part[2] += rs * z;
                     part[3] += a * z;
                     part[4] += a * (d * a);
-                    Zc[cl.t] = zp;
-                    Qc[cl.t] = __fmul_rn(dg[s], ap[s]);
-                    if (k > 0) Pc[cl.t] = pk;
+                    // only cells on the tile's faces are another tile's face neighbours
+                    if (m == 0 || m == 3 || bj == 0 || bj == 7 || bk == 0 || bk == 31) {
+                        Zc[cl.t] = zp;
+                        Qc[cl.t] = __fmul_rn(dg[s], ap[s]);
+                    }
                 }
             }
             stash_warp<kOneComps>(part, red, 0);
