@@ -403,52 +403,66 @@ __device__ __forceinline__ float heat_nt_hoisted(const hf_scene& S, const X& x, 
     return acc;
 }
 
-// heat.py:121-144 k_heat_diag: sum of the in-domain face diffusivities
-__device__ __forceinline__ float heat_diag_sum(const hf_scene& S, int i, int j, int k) {
-    const int n = S.n;
-    float s = 0.0f;
-    if (i > 0) s = __fadd_rn(s, S.hkx[uidx_(n, i, j, k)]);
-    if (i < n - 1) s = __fadd_rn(s, S.hkx[uidx_(n, i + 1, j, k)]);
-    if (j > 0) s = __fadd_rn(s, S.hky[vidx_(n, i, j, k)]);
-    if (j < n - 1) s = __fadd_rn(s, S.hky[vidx_(n, i, j + 1, k)]);
-    if (k > 0) s = __fadd_rn(s, S.hkz[widx_(n, i, j, k)]);
-    if (k < n - 1) s = __fadd_rn(s, S.hkz[widx_(n, i, j, k + 1)]);
-    return s;
-}
-
 // Set-up of one cell (heat.py:198-203 + k_heat_rhs/k_heat_diag; grid.py:238-248 mean removal + k_jacobi): returns
-// b, D, r for x0 (the advected T, or the previous pressure).
+// b, D, r for x0 (the advected T, or the previous pressure).  Every load comes first and stays in bounds (a missing
+// neighbour reads the cell itself), so they are in flight together; the sums then take the in-domain terms in the
+// reference's order (heat.py:121-144 k_heat_diag and heat_nt, or k_jacobi's face-fraction sum and lap_acc).
 template <bool HEAT>
 __device__ __forceinline__ void setup_cell(const hf_scene& S, const float* x, float mean, float hh, float c_dt,
                                            const Cell& c, float& b, float& d, float& r) {
-    const int n = S.n;
-    const float xc = x[c.t];
-    const Vec X{x};
+    const int n = S.n, nn = n * n, t = c.t, i = c.i, j = c.j, k = c.k;
+    const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
+    const int step[6] = {-nn, nn, -n, n, -1, 1};
+    const int fidx[6] = {uidx_(n, i, j, k), uidx_(n, i + 1, j, k), vidx_(n, i, j, k), vidx_(n, i, j + 1, k),
+                         widx_(n, i, j, k), widx_(n, i, j, k + 1)};
+    const float xc = x[t];
+    float xn[6], kf[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) xn[s] = x[in[s] ? t + step[s] : t];
     if (HEAT) {
-        b = S.hrhs[c.t];
-        if (S.cell_flags[c.t] & 1) {
+        const float* __restrict__ hk[3] = {S.hkx, S.hky, S.hkz};
+        const uint8_t* __restrict__ fl = S.cell_flags;
+        uint8_t fn[6];
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            kf[s] = __ldg(hk[s >> 1] + fidx[s]);
+            fn[s] = __ldg(fl + (in[s] ? t + step[s] : t));
+        }
+        b = S.hrhs[t];
+        if (fl[t] & 1) {
             d = 1.0f;
             r = __fsub_rn(b, xc);
         } else {
-            d = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(c_dt, heat_diag_sum(S, c.i, c.j, c.k))));
-            r = __fsub_rn(b, __fadd_rn(xc, __fmul_rn(c_dt, heat_nt(S, X, xc, c.t, c.i, c.j, c.k))));
+            float sd = 0.0f, nt = 0.0f;
+#pragma unroll
+            for (int s = 0; s < 6; ++s)
+                if (in[s]) sd = __fadd_rn(sd, kf[s]);
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                if (!in[s]) continue;
+                nt = __fadd_rn(nt, (fn[s] & 1) ? __fmul_rn(kf[s], xc) : __fmul_rn(kf[s], __fsub_rn(xc, xn[s])));
+            }
+            d = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(c_dt, sd)));
+            r = __fsub_rn(b, __fadd_rn(xc, __fmul_rn(c_dt, nt)));
         }
     } else {
-        b = S.rhs[c.t];
+        const float* __restrict__ af[3] = {S.ax, S.ay, S.az};
+#pragma unroll
+        for (int s = 0; s < 6; ++s) kf[s] = __ldg(af[s >> 1] + fidx[s]);
+        b = S.rhs[t];
         if (mean != 0.0f) {
             b = __fsub_rn(b, mean);
-            S.rhs[c.t] = b;
+            S.rhs[t] = b;
         }
-        const int i = c.i, j = c.j, k = c.k;
-        float sa = 0.0f;
-        if (i > 0) sa = __fadd_rn(sa, S.ax[uidx_(n, i, j, k)]);
-        if (i < n - 1) sa = __fadd_rn(sa, S.ax[uidx_(n, i + 1, j, k)]);
-        if (j > 0) sa = __fadd_rn(sa, S.ay[vidx_(n, i, j, k)]);
-        if (j < n - 1) sa = __fadd_rn(sa, S.ay[vidx_(n, i, j + 1, k)]);
-        if (k > 0) sa = __fadd_rn(sa, S.az[widx_(n, i, j, k)]);
-        if (k < n - 1) sa = __fadd_rn(sa, S.az[widx_(n, i, j, k + 1)]);
+        float sa = 0.0f, acc = 0.0f;
+#pragma unroll
+        for (int s = 0; s < 6; ++s)
+            if (in[s]) sa = __fadd_rn(sa, kf[s]);
+#pragma unroll
+        for (int s = 0; s < 6; ++s)
+            if (in[s]) acc = __fadd_rn(acc, __fmul_rn(kf[s], __fsub_rn(xc, xn[s])));
         d = __fdiv_rn(hh, maxf_(sa, 1.0e-12f));
-        r = __fsub_rn(b, __fdiv_rn(lap_acc(S, X, xc, c.t, i, j, k), hh));
+        r = __fsub_rn(b, __fdiv_rn(acc, hh));
     }
 }
 
