@@ -342,6 +342,20 @@ __global__ void __launch_bounds__(kThreads, 4) k_advect_T(const hf_scene* __rest
         if (t >= N) break;
         int i, j, k;
         cell_ijk(t, n, i, j, k);
+        // the heat rhs's flags and face diffusivities are loaded first (in bounds: a missing neighbour reads the cell
+        // itself, the face lattices have n + 1 layers), so they arrive while the back-trace is computed
+        const int nbr[6] = {t - n * n, t + n * n, t - n, t + n, t - 1, t + 1};
+        const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
+        const uint8_t fc = fl[t];
+        uint8_t fn[6];
+        float kf[6];
+        const float* hk[6] = {S.hkx + uidx(n, i, j, k), S.hkx + uidx(n, i + 1, j, k), S.hky + vidx(n, i, j, k),
+                              S.hky + vidx(n, i, j + 1, k), S.hkz + widx(n, i, j, k), S.hkz + widx(n, i, j, k + 1)};
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            fn[s] = fl[in[s] ? nbr[s] : t];
+            kf[s] = *hk[s];
+        }
         float out;
         if (S.alpha_s[t] > 0.5f) {
             out = Tw[t];
@@ -355,20 +369,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_advect_T(const hf_scene* __rest
         T2[t] = out;
         // heat rhs: tfix on fixed cells, else T2 + dt/h^2 * sum over fixed neighbours of kappa_f * tfix
         float rhs;
-        if (fl[t] & 1) {
+        if (fc & 1) {
             rhs = S.tfix[t];
         } else {
             float acc = 0.0f;
-            const int nbr[6] = {t - n * n, t + n * n, t - n, t + n, t - 1, t + 1};
-            const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
-            const float kf[6] = {in[0] ? S.hkx[uidx(n, i, j, k)] : 0.0f, in[1] ? S.hkx[uidx(n, i + 1, j, k)] : 0.0f,
-                                 in[2] ? S.hky[vidx(n, i, j, k)] : 0.0f, in[3] ? S.hky[vidx(n, i, j + 1, k)] : 0.0f,
-                                 in[4] ? S.hkz[widx(n, i, j, k)] : 0.0f, in[5] ? S.hkz[widx(n, i, j, k + 1)] : 0.0f};
 #pragma unroll
             for (int s = 0; s < 6; ++s) {
                 if (!in[s]) continue;
-                const int nb = nbr[s];
-                if (fl[nb] & 1) acc = __fadd_rn(acc, __fmul_rn(kf[s], S.tfix[nb]));
+                if (fn[s] & 1) acc = __fadd_rn(acc, __fmul_rn(kf[s], S.tfix[nbr[s]]));
             }
             rhs = __fadd_rn(out, __fmul_rn(c_dt, acc));
         }
