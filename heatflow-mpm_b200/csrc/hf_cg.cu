@@ -608,6 +608,13 @@ constexpr int kHeatSlotFloats = kSlotFloats + kBF / 4;             // 9344 float
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
+// The first 128-byte aligned float of the dynamic shared memory (TMA destinations), derived from raw by pointer
+// arithmetic so that the compiler keeps the shared address space: a round trip through an integer would turn every
+// access to the boxes into a generic load or store.
+__device__ __forceinline__ float* align128_shared(float* raw) {
+    return raw + ((128u - (smem_addr(raw) & 127u)) & 127u) / 4u;
+}
+
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
@@ -1115,7 +1122,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
     __shared__ int s_any;
     __shared__ __align__(8) unsigned long long mbar[2];
     extern __shared__ __align__(128) float sm_raw[];
-    float* slots = TMA ? reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127) : nullptr;
+    float* slots = TMA ? align128_shared(sm_raw) : nullptr;
     unsigned ph[2] = {0u, 0u};
     if (TMA && threadIdx.x == 0) {
         mbar_init(&mbar[0], 1);
@@ -1155,7 +1162,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     constexpr int CPT = 4 * MAXC;   // cells per thread
     extern __shared__ __align__(128) float sm_raw[];
     // TMA destinations must be 128-byte aligned: the launch adds 128 bytes of slack
-    float* sm_boxes = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
+    float* sm_boxes = align128_shared(sm_raw);
     __shared__ double red[kRedComps * 32];
     __shared__ LocalScene Ls;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
@@ -1455,7 +1462,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     constexpr int CPT = 4 * MAXC;
     constexpr int SLOT = HEAT ? kHeatSlotFloats : kSlotFloats;
     extern __shared__ __align__(128) float sm_raw[];
-    float* sm_boxes = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
+    float* sm_boxes = align128_shared(sm_raw);
     __shared__ double red[kRedComps * 32];
     __shared__ LocalScene Ls;
     __shared__ __align__(8) unsigned long long mbar[4 * 3];
@@ -1888,7 +1895,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
               double dt_d, Workspace ws, const __grid_constant__ TileMaps maps) {
     constexpr int CPT = 4 * MAXC;
     extern __shared__ __align__(128) float sm_raw[];
-    float* sm_slots = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~(uintptr_t)127);
+    float* sm_slots = align128_shared(sm_raw);
     __shared__ double red[kOneComps * 3 * 32];   // five partials per warp (the set-up: three of up to three tiles)
     __shared__ unsigned hmask_s[1024];
     __shared__ TileItem my_s[4 * 3];
