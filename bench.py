@@ -232,16 +232,53 @@ def run_reference(args):
 
 # --------------------------------------------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock and throttle reasons of GPU `index` during the timed region, read through NVML (nvidia_ml_py) every
+    ~2 ms on a thread, so that a region of a few ms still holds samples; nvidia-smi -lms 50 where NVML is unavailable.
+    Reads only: no clock or other GPU setting is changed."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index):
         self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.f = None
         self.p = None
+        self.thread = None
+        self.samples = []
+
+    def _poll(self, nvml, handle, stop):
+        reasons_fn = getattr(nvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not stop.is_set():
+            try:
+                sm = nvml.nvmlDeviceGetClockInfo(handle, nvml.NVML_CLOCK_SM)
+                mx = nvml.nvmlDeviceGetMaxClockInfo(handle, nvml.NVML_CLOCK_SM)
+                rs = reasons_fn(handle)
+            except Exception:  # noqa: BLE001 - a failed read ends the sampling, it does not end the bench
+                break
+            self.samples.append((time.perf_counter(), float(sm), float(mx), int(rs)))
+            time.sleep(0.002)
 
     def start(self):
+        import threading
+        try:
+            import pynvml as nvml
+            nvml.nvmlInit()
+            handle = nvml.nvmlDeviceGetHandleByIndex(self.index)
+        except Exception:  # noqa: BLE001 - no NVML: fall back to nvidia-smi
+            nvml = None
+        if nvml is not None:
+            self.stop_evt = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(nvml, handle, self.stop_evt), daemon=True)
+            self.thread.start()
+            t_wait = time.perf_counter()
+            while not self.samples and self.thread.is_alive() and time.perf_counter() - t_wait < 2.0:
+                time.sleep(0.001)
+            self.t0 = time.perf_counter()
+            return
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader",
                                        "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
@@ -249,6 +286,19 @@ class ClockSampler:
             self.p = None
 
     def stop(self):
+        if self.thread is not None:
+            t1 = time.perf_counter()
+            self.stop_evt.set()
+            self.thread.join(timeout=5)
+            inside = [s for s in self.samples if self.t0 <= s[0] <= t1]
+            if not inside:
+                before = [s for s in self.samples if s[0] <= t1]
+                inside = before[-1:]
+            if not inside:
+                return None
+            reasons = sorted(nm for nm, bit in self.REASON_BITS.items() if any(s[3] & bit for s in inside))
+            return {"sm_mhz": statistics.median(s[1] for s in inside), "sm_max_mhz": max(s[2] for s in inside),
+                    "reasons": reasons, "samples": len(inside), "source": "nvml"}
         if self.p is None:
             return None
         self.p.terminate()
@@ -272,7 +322,8 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvidia-smi"}
 
 
 # --------------------------------------------------------------------------------------------------- bytes
