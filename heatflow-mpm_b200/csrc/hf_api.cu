@@ -105,7 +105,7 @@ Layout layout(int S, int C, int T) {
     o = align_up(o + sizeof(int) * (size_t)(S + 1), 256);
     L.maps = o;                      // kMapsPerScene TMA descriptors per scene (128 bytes each)
     o = align_up(o + sizeof(CUtensorMap) * hf::kMapsPerScene * (size_t)S, 256);
-    L.partA = o;                     // 5 doubles per tile (3 used by the classic variants)
+    L.partA = o;                     // 5 doubles per tile, component-major (3 components used by the classic variants)
     o = align_up(o + sizeof(double) * 5 * (size_t)T, 256);
     L.partB = o;
     o = align_up(o + sizeof(double) * 5 * (size_t)T, 256);
@@ -129,6 +129,7 @@ hf::Workspace workspace(const hf_plan* p) {
     w.partA = reinterpret_cast<double*>(b + L.partA);
     w.partB = reinterpret_cast<double*>(b + L.partB);
     w.mean_part = reinterpret_cast<double*>(b + L.mean_part);
+    w.tiles = p->num_tiles;
     return w;
 }
 

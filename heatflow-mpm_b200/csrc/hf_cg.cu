@@ -76,12 +76,13 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& epoch, int
     return *(volatile int*)err == 0;
 }
 
-// Sum of a scene's partials (item c, component comp[q] at buf[STRIDE * c + comp[q]]) in a fixed tree: the first 256
-// threads stride over the items in order, warp butterfly, then 8 warps in order.  Every block computing it obtains the
-// same bits.  STRIDE is 3 for the tile partials and 1 for the per-chunk rhs sums.
-template <int K, int STRIDE = 3, int U = 4>
+// Sum of a scene's partials (item c, component comp[q] at buf[comp[q] * cs + c]: component-major, so that a warp's
+// loads of one component are contiguous) in a fixed tree: the first 256 threads stride over the items in order, warp
+// butterfly, then 8 warps in order.  Every block computing it obtains the same bits.  cs is the plan's tile count for
+// the tile partials (three components, see part_idx) and 0 for the per-chunk rhs sums (one component).
+template <int K, int U = 4>
 __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b, int e, const int (&comp)[K],
-                                           double (&tot)[K], double* red) {
+                                           double (&tot)[K], double* red, int cs) {
     static_assert(K <= kRedComps, "red holds kRedComps components");
 #pragma unroll
     for (int q = 0; q < K; ++q) tot[q] = 0.0;
@@ -94,7 +95,7 @@ __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
-                for (int q = 0; q < K; ++q) v[u][q] = c + u * kThreads < e ? buf[STRIDE * (c + u * kThreads) + comp[q]] : 0.0;
+                for (int q = 0; q < K; ++q) v[u][q] = c + u * kThreads < e ? buf[comp[q] * cs + c + u * kThreads] : 0.0;
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -118,87 +119,6 @@ __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b
         double s = 0.0;
 #pragma unroll
         for (int q = 0; q < kThreads / 32; ++q) s += red[c * 32 + q];
-        tot[c] = s;
-    }
-}
-
-// scene_sums for components comp0 .. comp0 + K - 1 with each component on its own 256 threads (blockDim >= 256 K): the
-// threads 256 q .. 256 q + 255 run exactly the first 256 threads' part of scene_sums for component q, so the sums are
-// bit-identical to scene_sums', with a quarter of the loads and registers per thread.
-template <int K, int STRIDE = 3>
-__device__ __forceinline__ void scene_sums_wide(const double* __restrict__ buf, int b, int e, int comp0, double (&tot)[K],
-                                                double* red) {
-    static_assert(K <= kRedComps, "red holds kRedComps components");
-    const int q = threadIdx.x >> 8, lt = threadIdx.x & 255;
-    double acc = 0.0;
-    if (q < K) {
-        const int cq = comp0 + q;
-        for (int c = b + lt; c < e; c += 4 * kThreads) {
-            double v[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = c + u * kThreads < e ? buf[STRIDE * (c + u * kThreads) + cq] : 0.0;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) acc += v[u];
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    }
-    const int lane = threadIdx.x & 31, wq = lt >> 5;
-    __syncthreads();
-    if (q < K && lane == 0) red[q * 32 + wq] = acc;
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-        double s = 0.0;
-#pragma unroll
-        for (int w = 0; w < kThreads / 32; ++w) s += red[c * 32 + w];
-        tot[c] = s;
-    }
-}
-
-// scene_sums for K components spread over G groups of 256 threads (blockDim >= 256 G): group q sums components q,
-// q + G, q + 2 G, ... each exactly as scene_sums' first 256 threads do (the same tree, the same bits), with ceil(K / G)
-// of them per thread, U partials of each loaded at a time.
-template <int K, int STRIDE, int G = 3, int U = 4>
-__device__ __forceinline__ void scene_sums_3g(const double* __restrict__ buf, int b, int e, double (&tot)[K],
-                                              double* red) {
-    constexpr int KPT = (K + G - 1) / G;
-    const int q = threadIdx.x >> 8, lt = threadIdx.x & 255;
-    double acc[KPT];
-#pragma unroll
-    for (int j = 0; j < KPT; ++j) acc[j] = 0.0;
-    if (q < G) {
-        for (int c = b + lt; c < e; c += U * kThreads) {
-            double v[KPT][U];
-#pragma unroll
-            for (int j = 0; j < KPT; ++j)
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    v[j][u] = q + G * j < K && c + u * kThreads < e ? buf[STRIDE * (c + u * kThreads) + q + G * j] : 0.0;
-#pragma unroll
-            for (int j = 0; j < KPT; ++j)
-#pragma unroll
-                for (int u = 0; u < U; ++u) acc[j] += v[j][u];
-        }
-#pragma unroll
-        for (int j = 0; j < KPT; ++j) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
-        }
-    }
-    const int lane = threadIdx.x & 31, wq = lt >> 5;
-    __syncthreads();
-    if (q < G && lane == 0) {
-#pragma unroll
-        for (int j = 0; j < KPT; ++j)
-            if (q + G * j < K) red[(q + G * j) * 32 + wq] = acc[j];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-        double s = 0.0;
-#pragma unroll
-        for (int w = 0; w < kThreads / 32; ++w) s += red[c * 32 + w];
         tot[c] = s;
     }
 }
@@ -232,7 +152,7 @@ __device__ __forceinline__ void group_sum(double (&v)[K], double* red) {
 // group_sum in two steps, so that a thread holds the partials of one tile at a time: stash_warp reduces K values over the
 // warp (the same butterfly) and lane 0 parks them in red[(c0 + c) * 32 + warp]; after every tile's stash,
 // publish_group (thread lt == 0 of each 256-thread group) adds the group's 8 warps in order -- group_sum's tree, the
-// same bits -- and writes the tile partials to buf[3 * tile + c] (3 components per tile).  red must not be read by
+// same bits -- and writes the tile partials to buf[c * tiles + tile] (3 components, component-major).  red must not be read by
 // another phase in between (the caller's barriers see to that).
 template <int K>
 __device__ __forceinline__ void stash_warp(double (&v)[K], double* red, int c0) {
@@ -249,7 +169,7 @@ __device__ __forceinline__ void stash_warp(double (&v)[K], double* red, int c0) 
 
 template <int MAXC>
 __device__ __forceinline__ void publish_group(const double* red, double* __restrict__ buf, int first_tile, int groups,
-                                              int c_end) {
+                                              int c_end, int tiles) {
     __syncthreads();
     if ((threadIdx.x & 255) == 0) {
         const int g0 = (threadIdx.x >> 5);   // first warp of this group
@@ -262,16 +182,17 @@ __device__ __forceinline__ void publish_group(const double* red, double* __restr
                 double s = 0.0;
 #pragma unroll
                 for (int w = 0; w < 8; ++w) s += red[(3 * q + comp) * 32 + g0 + w];
-                buf[3 * c + comp] = s;
+                buf[comp * tiles + c] = s;
             }
         }
     }
 }
 
-// One partial per 256-thread group (the single-reduction CG's five components, stride K): after stash_warp<K>(v, red,
-// 0) in every warp, thread lt == 0 of each group adds its 8 warps in order and writes buf[K * unit + comp].
+// One partial per 256-thread group (the single-reduction CG's five components), stored component-major so that a
+// warp's loads of one component are contiguous: after stash_warp<K>(v, red, 0) in every warp, thread lt == 0 of each
+// group adds its 8 warps in order and writes buf[comp * units + unit].
 template <int K>
-__device__ __forceinline__ void publish_unit(const double* red, double* __restrict__ buf, int unit) {
+__device__ __forceinline__ void publish_unit(const double* red, double* __restrict__ buf, int unit, int units) {
     __syncthreads();
     if ((threadIdx.x & 255) == 0) {
         const int g0 = (threadIdx.x >> 5);
@@ -280,8 +201,65 @@ __device__ __forceinline__ void publish_unit(const double* red, double* __restri
             double s = 0.0;
 #pragma unroll
             for (int w = 0; w < 8; ++w) s += red[comp * 32 + g0 + w];
-            buf[K * unit + comp] = s;
+            buf[comp * units + unit] = s;
         }
+    }
+}
+
+// The K sums of the groups' component-major partials (publish_unit), in every thread of the block.  The tree is
+// scene_sums_3g's: the G groups of 256 threads take components q, q + G, ...; thread lt adds units lt, lt + 256, ...
+// in order (absent ones as +0.0), then the warp butterfly and the 8 warps in order.  unit_loads issues the loads of
+// the thread's first U units (so that the caller can put them ahead of other memory traffic); unit_sums adds them,
+// then any further units, and reduces.
+template <int K, int G, int U>
+__device__ __forceinline__ void unit_loads(const double* __restrict__ buf, int units, double (&v)[K][U]) {
+    constexpr int KPT = (K + G - 1) / G;
+    const int q = threadIdx.x >> 8, lt = threadIdx.x & 255;
+#pragma unroll
+    for (int j = 0; j < KPT; ++j)
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            v[j][u] = q < G && q + G * j < K && lt + u * kThreads < units ? buf[(q + G * j) * units + lt + u * kThreads] : 0.0;
+}
+
+template <int K, int G, int U>
+__device__ __forceinline__ void unit_sums(const double* __restrict__ buf, int units, const double (&v)[K][U],
+                                          double (&tot)[K], double* red) {
+    constexpr int KPT = (K + G - 1) / G;
+    const int q = threadIdx.x >> 8, lt = threadIdx.x & 255;
+    double acc[KPT];
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        acc[j] = 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc[j] += v[j][u];
+    }
+    if (q < G) {
+        for (int c = lt + U * kThreads; c < units; c += kThreads) {
+#pragma unroll
+            for (int j = 0; j < KPT; ++j)
+                if (q + G * j < K) acc[j] += buf[(q + G * j) * units + c];
+        }
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+        }
+    }
+    const int lane = threadIdx.x & 31, wq = lt >> 5;
+    __syncthreads();
+    if (q < G && lane == 0) {
+#pragma unroll
+        for (int j = 0; j < KPT; ++j)
+            if (q + G * j < K) red[(q + G * j) * 32 + wq] = acc[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) s += red[c * 32 + w];
+        tot[c] = s;
     }
 }
 
@@ -703,7 +681,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             // the pressure rhs mean (grid.py:238-241) from the divergence stage's chunk sums
             double m[1];
             const int comp[1] = {0};
-            scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[s], ws.chunk_begin[s + 1], comp, m, red);
+            scene_sums<1>(ws.mean_part, ws.chunk_begin[s], ws.chunk_begin[s + 1], comp, m, red, 0);
             const int n = scenes[s].n;
             if (threadIdx.x == 0) loc[q].mean = (double)__double2float_rn(m[0] / ((double)n * n * n));
         } else if (threadIdx.x == 0) {
@@ -735,9 +713,9 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
         }
         group_sum<3>(part, red);
         if (lt == 0) {
-            bufB[3 * c] = part[0];
-            bufB[3 * c + 1] = part[1];
-            bufB[3 * c + 2] = part[2];
+            bufB[c] = part[0];
+            bufB[1 * ws.tiles + c] = part[1];
+            bufB[2 * ws.tiles + c] = part[2];
         }
     }
     if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
@@ -746,7 +724,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
         const int b = ws.tile_begin[s], e = ws.tile_begin[s + 1];
         double tot[3];
         const int comp[3] = {0, 1, 2};
-        scene_sums<3>(bufB, b, e, comp, tot, red);
+        scene_sums<3>(bufB, b, e, comp, tot, red, ws.tiles);
         if (threadIdx.x == 0) {
             const hf_scene& S = scenes[s];
             const double mean = loc[q].mean;
@@ -824,7 +802,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
                     part[0] += (double)pc * (double)ap;
                 }
                 group_sum<1>(part, red);   // its __syncthreads also ends every read of the slot
-                if (lt == 0) bufA[3 * c] = part[0];
+                if (lt == 0) bufA[c] = part[0];
             };
             pipelined_tiles(first, tile_hi, nlb, loc, scene_lo, tiles, slots, mbar, ph, ws.err, issue, work);
         }
@@ -862,7 +840,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
                 part[0] += (double)pc[m] * (double)ap[m];
             }
             group_sum<1>(part, red);
-            if (lt == 0) bufA[3 * c] = part[0];
+            if (lt == 0) bufA[c] = part[0];
         }
         if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
         for (int q = 0; q < ns; ++q) {
@@ -870,7 +848,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             const int s = scene_lo + q;
             double tot[1];
             const int comp[1] = {0};
-            scene_sums<1>(bufA, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
+            scene_sums<1>(bufA, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red, ws.tiles);
             if (threadIdx.x == 0) {
                 loc[q].pAp = tot[0];
                 loc[q].alpha = __double2float_rn(loc[q].rz / tot[0]);
@@ -918,8 +896,8 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
                 }
                 group_sum<2>(part, red);
                 if (lt == 0) {
-                    bufB[3 * c + 1] = part[0];
-                    bufB[3 * c + 2] = part[1];
+                    bufB[1 * ws.tiles + c] = part[0];
+                    bufB[2 * ws.tiles + c] = part[1];
                 }
             };
             pipelined_tiles(first, tile_hi, nlb, loc, scene_lo, tiles, slots, mbar, ph, ws.err, issue, work);
@@ -959,8 +937,8 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             }
             group_sum<2>(part, red);
             if (lt == 0) {
-                bufB[3 * c + 1] = part[0];
-                bufB[3 * c + 2] = part[1];
+                bufB[1 * ws.tiles + c] = part[0];
+                bufB[2 * ws.tiles + c] = part[1];
             }
         }
         if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
@@ -969,7 +947,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             const int s = scene_lo + q;
             double tot[2];
             const int comp[2] = {1, 2};
-            scene_sums<2>(bufB, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
+            scene_sums<2>(bufB, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red, ws.tiles);
             if (threadIdx.x == 0) update_scalars(loc[q], HEAT, tot[0], tot[1], loc[q].kbase + kit);
         }
         if (threadIdx.x == 0) {
@@ -1006,7 +984,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             part[0] += rt * rt;
         }
         group_sum<1>(part, red);
-        if (lt == 0) bufA[3 * c + 1] = part[0];
+        if (lt == 0) bufA[1 * ws.tiles + c] = part[0];
     }
     if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
     for (int q = 0; q < ns; ++q) {
@@ -1014,7 +992,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
         const int s = scene_lo + q;
         double tot[1];
         const int comp[1] = {1};
-        scene_sums<1>(bufA, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
+        scene_sums<1>(bufA, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red, ws.tiles);
         if (threadIdx.x == 0) {
             LocalScene& L = loc[q];
             L.true_rr = tot[0];
@@ -1059,8 +1037,8 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
         }
         group_sum<2>(part, red);
         if (lt == 0) {
-            bufB[3 * c + 1] = part[0];
-            bufB[3 * c + 2] = part[1];
+            bufB[1 * ws.tiles + c] = part[0];
+            bufB[2 * ws.tiles + c] = part[1];
         }
     }
     if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
@@ -1069,7 +1047,7 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
         const int s = scene_lo + q;
         double tot[2];
         const int comp[2] = {1, 2};
-        scene_sums<2>(bufB, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red);
+        scene_sums<2>(bufB, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red, ws.tiles);
         if (threadIdx.x == 0) {
             LocalScene& L = loc[q];
             L.rr = tot[0];
@@ -1206,7 +1184,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     if (!HEAT) {
         double mm[1];
         const int comp[1] = {0};
-        scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red);
+        scene_sums<1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red, 0);
         mean = __double2float_rn(mm[0] / ((double)n * n * n));
     }
 #pragma unroll
@@ -1232,9 +1210,9 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         group_sum<3>(part, red);
         const int c = c0 + g + groups * q;
         if (lt == 0 && have[q]) {
-            bufB[3 * c] = part[0];
-            bufB[3 * c + 1] = part[1];
-            bufB[3 * c + 2] = part[2];
+            bufB[c] = part[0];
+            bufB[1 * ws.tiles + c] = part[1];
+            bufB[2 * ws.tiles + c] = part[2];
         }
     }
     // the face fractions of the tiles stay in shared memory for the whole solve
@@ -1262,7 +1240,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     {
         double tot[3];
         const int comp[3] = {0, 1, 2};
-        scene_sums<3>(bufB, cb, ce, comp, tot, red);
+        scene_sums<3>(bufB, cb, ce, comp, tot, red, ws.tiles);
         if (threadIdx.x == 0) {
             init_scalars(Ls, S, HEAT, tot, N);
             Ls.mean = (double)mean;
@@ -1371,13 +1349,13 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             }
             group_sum<1>(part, red);
             const int c = c0 + g + groups * q;
-            if (lt == 0 && have[q]) bufA[3 * c] = part[0];
+            if (lt == 0 && have[q]) bufA[c] = part[0];
         }
         if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
         {
             double tot[1];
             const int comp[1] = {0};
-            scene_sums<1>(bufA, cb, ce, comp, tot, red);
+            scene_sums<1>(bufA, cb, ce, comp, tot, red, ws.tiles);
             if (threadIdx.x == 0) {
                 Ls.pAp = tot[0];
                 Ls.alpha = __double2float_rn(Ls.rz / tot[0]);
@@ -1404,15 +1382,15 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             group_sum<2>(part, red);
             const int c = c0 + g + groups * q;
             if (lt == 0 && have[q]) {
-                bufB[3 * c + 1] = part[0];
-                bufB[3 * c + 2] = part[1];
+                bufB[1 * ws.tiles + c] = part[0];
+                bufB[2 * ws.tiles + c] = part[1];
             }
         }
         if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
         {
             double tot[2];
             const int comp[2] = {1, 2};
-            scene_sums<2>(bufB, cb, ce, comp, tot, red);
+            scene_sums<2>(bufB, cb, ce, comp, tot, red, ws.tiles);
             if (threadIdx.x == 0) update_scalars(Ls, HEAT, tot[0], tot[1], kit);
             __syncthreads();
         }
@@ -1524,7 +1502,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     if (!HEAT) {
         double mm[1];
         const int comp[1] = {0};
-        scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red);
+        scene_sums<1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red, 0);
         mean = __double2float_rn(mm[0] / ((double)n * n * n));
     }
     {
@@ -1555,9 +1533,9 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         for (int q = 0; q < MAXC; ++q) {
             const int c = c0 + g + groups * q;
             if (lt == 0 && have[q]) {
-                bufB[3 * c] = part[3 * q];
-                bufB[3 * c + 1] = part[3 * q + 1];
-                bufB[3 * c + 2] = part[3 * q + 2];
+                bufB[c] = part[3 * q];
+                bufB[1 * ws.tiles + c] = part[3 * q + 1];
+                bufB[2 * ws.tiles + c] = part[3 * q + 2];
             }
         }
     }
@@ -1591,7 +1569,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     {
         double tot[3];
         const int comp[3] = {0, 1, 2};
-        scene_sums<3>(bufB, cb, ce, comp, tot, red);
+        scene_sums<3>(bufB, cb, ce, comp, tot, red, ws.tiles);
         if (threadIdx.x == 0) {
             init_scalars(Ls, S, HEAT, tot, N);
             Ls.mean = (double)mean;
@@ -1701,14 +1679,14 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
 #pragma unroll
             for (int q = 0; q < MAXC; ++q) {
                 const int c = c0 + g + groups * q;
-                if (lt == 0 && have[q]) bufA[3 * c] = part[q];
+                if (lt == 0 && have[q]) bufA[c] = part[q];
             }
         }
         if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
         {
             double tot[1];
             const int comp[1] = {0};
-            scene_sums<1>(bufA, cb, ce, comp, tot, red);
+            scene_sums<1>(bufA, cb, ce, comp, tot, red, ws.tiles);
             if (threadIdx.x == 0) {
                 Ls.pAp = tot[0];
                 Ls.alpha = __double2float_rn(Ls.rz / tot[0]);
@@ -1742,8 +1720,8 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             for (int q = 0; q < MAXC; ++q) {
                 const int c = c0 + g + groups * q;
                 if (lt == 0 && have[q]) {
-                    bufB[3 * c + 1] = part[2 * q];
-                    bufB[3 * c + 2] = part[2 * q + 1];
+                    bufB[1 * ws.tiles + c] = part[2 * q];
+                    bufB[2 * ws.tiles + c] = part[2 * q + 1];
                 }
             }
         }
@@ -1753,7 +1731,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
         {
             double tot[2];
             const int comp[2] = {1, 2};
-            scene_sums<2>(bufB, cb, ce, comp, tot, red);
+            scene_sums<2>(bufB, cb, ce, comp, tot, red, ws.tiles);
             if (threadIdx.x == 0) update_scalars(Ls, HEAT, tot[0], tot[1], kit);
             __syncthreads();
         }
@@ -1962,7 +1940,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     {
         double mm[1];
         const int comp[1] = {0};
-        scene_sums<1, 1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red);
+        scene_sums<1>(ws.mean_part, ws.chunk_begin[sidx], ws.chunk_begin[sidx + 1], comp, mm, red, 0);
         mean = __double2float_rn(mm[0] / ((double)n * n * n));
     }
     {
@@ -1992,7 +1970,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             }
             stash_warp<3>(part, red, 3 * q);
         }
-        publish_group<MAXC>(red, bufB, c0 + g, groups, c1);
+        publish_group<MAXC>(red, bufB, c0 + g, groups, c1, ws.tiles);
     }
     // the tiles' face fractions stay in shared memory for the whole solve
     if (lt == 0) {
@@ -2012,7 +1990,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     {
         double tot[3];
         const int comp[3] = {0, 1, 2};
-        scene_sums<3>(bufB, cb, ce, comp, tot, red);
+        scene_sums<3>(bufB, cb, ce, comp, tot, red, ws.tiles);
         if (threadIdx.x == 0) {
             init_scalars(Ls, S, false, tot, N);
             Ls.mean = (double)mean;
@@ -2037,7 +2015,15 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 tma_load_3d(slot_of(q), &maps.p0, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
             }
         }
-        // k >= 1: the neighbours' z', q (cp.async), in flight during the scene sums
+        // k >= 1: the loads of this iteration's scene sums first, then the neighbours' z', q (cp.async), in flight
+        // while the sums are formed
+        double sv[kOneComps][2];
+        if (k > 0) {
+            if (groups >= 2)
+                unit_loads<kOneComps, 2, 2>(prev ? bufB : bufA, units, sv);
+            else
+                unit_loads<kOneComps, 1, 2>(prev ? bufB : bufA, units, sv);
+        }
         if (k > 0) {
             const float* Zp = prev ? S.cg_z : S.cg_r;
             const float* Qp = prev ? S.hdiag : S.cg_Ap;
@@ -2059,44 +2045,41 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             asm volatile("cp.async.commit_group;" ::: "memory");
         }
         float alpha = 0.0f, beta = 0.0f;
+        bool live = true;   // k = 0 runs only when the set-up left the scene live
         if (k > 0) {
             double tot[kOneComps];
-            // pAp, rr, rz, Ap.z, Ap.D.Ap of iteration k - 1: the groups' partials in group order
-            if (MAXC < 3 && blockDim.x >= 3 * kThreads) {
-                scene_sums_3g<kOneComps, kOneComps, 3, 2>(prev ? bufB : bufA, 0, units, tot, red);
-            } else if (blockDim.x >= 2 * kThreads) {
-                scene_sums_3g<kOneComps, kOneComps, 2, 2>(prev ? bufB : bufA, 0, units, tot, red);
-            } else {
-                const int comp[kOneComps] = {0, 1, 2, 3, 4};
-                scene_sums<kOneComps, kOneComps, 1>(prev ? bufB : bufA, 0, units, comp, tot, red);
+            // pAp, rr, rz, Ap.z, Ap.D.Ap of iteration k - 1: the groups' partials in group order, in every thread
+            if (groups >= 2)
+                unit_sums<kOneComps, 2, 2>(prev ? bufB : bufA, units, sv, tot, red);
+            else
+                unit_sums<kOneComps, 1, 2>(prev ? bufB : bufA, units, sv, tot, red);
+            // every thread derives the same test and scalars from the same sums (no broadcast through shared memory):
+            // the classic test on r_{k-1} (formed in iteration k - 1); converged -> x_{k-1} is the solution
+            const double pAp = tot[0], rr = tot[1], rz = tot[2];
+            const bool above = rr > Ls.atol_sq;
+            live = above && isfinite(rr) && (k - 1) < Ls.maxit;
+            if (live) {
+                const double a = rz / pAp;
+                const double rz_next = rz - 2.0 * a * tot[3] + a * a * tot[4];
+                alpha = __double2float_rn(a);
+                beta = __double2float_rn(rz_next / rz);
             }
             if (threadIdx.x == 0) {
-                // the classic test on r_{k-1} (formed in iteration k - 1): converged -> x_{k-1} is the solution
-                const double pAp = tot[0], rr = tot[1], rz = tot[2];
                 Ls.iters = k - 1;
                 Ls.rr = rr;
                 Ls.rz = rz;
                 Ls.pAp = pAp;
-                const bool above = rr > Ls.atol_sq;
                 if (!isfinite(rr)) Ls.status |= HF_SCENE_NONFINITE;
-                const bool live = above && isfinite(rr) && (k - 1) < Ls.maxit;
                 if (!live && above && isfinite(rr)) Ls.status |= HF_SCENE_PRESSURE_MAXITER;
                 Ls.live = live;
-                if (live) {
-                    const double a = rz / pAp;
-                    const double rz_next = rz - 2.0 * a * tot[3] + a * a * tot[4];
-                    Ls.alpha = __double2float_rn(a);
-                    Ls.beta = __double2float_rn(rz_next / rz);
-                }
+                Ls.alpha = alpha;
+                Ls.beta = beta;
             }
-            __syncthreads();
-            alpha = Ls.alpha;
-            beta = Ls.beta;
         }
         if (k == 0) wait_boxes();
         if (k > 0) asm volatile("cp.async.wait_all;" ::: "memory");
         asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory");
-        if (!Ls.live) break;
+        if (!live) break;
         if (k > 0) {
             // p_k everywhere in the boxes by one formula: z = z' - alpha q, p = z + beta p_{k-1}; own cells also
             // advance x and r
@@ -2165,7 +2148,7 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 }
             }
             stash_warp<kOneComps>(part, red, 0);
-            publish_unit<kOneComps>(red, cur ? bufB : bufA, unit);
+            publish_unit<kOneComps>(red, cur ? bufB : bufA, unit, units);
         }
         if (!grid_barrier(bar, epoch, ws.err, gridDim.x)) goto finish;
     }

@@ -28,9 +28,11 @@ struct Workspace {
     int* tile_begin;        // [S+1] first tile of every scene in the tile table
     const CUtensorMap* maps;  // [kMapsPerScene S] per scene: the stencil boxes z, p_0, p_1, alpha_f x, alpha_f y (cells),
                               // alpha_f z (cells); then tile boxes of x (p), p_0, p_1, r, Ap, D
-    double* partA;          // [3*T] per-tile fp64 partials of CG phase A
-    double* partB;          // [3*T] per-tile fp64 partials of the CG set-up and phase B
+    double* partA;          // [3 T] per-tile fp64 partials of CG phase A, component-major: component c of tile t at
+                            // c * tiles + t (the single-reduction kernel: 5 components per 256-thread group)
+    double* partB;          // [3 T] per-tile fp64 partials of the CG set-up and phase B (same layout)
     double* mean_part;      // [C] per-chunk fp64 sums of the pressure rhs
+    int tiles;              // T: tiles of the plan, the component stride of partA / partB
 };
 
 // TMA descriptors of the tiled pressure stencil (resident CG): z, both search-direction buffers, alpha_f x (the u
