@@ -73,6 +73,8 @@ int device_info(DeviceInfo** out) {
         HF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_pressure_tma, hf::pcg_kernel(false, true), hf::kThreads,
                                                               hf::pcg_stream_smem(true)),
                 "occupancy");
+        HF_CUDA(cudaFuncSetAttribute(hf::k_face_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hf::face_tile_smem()),
+                "smem attribute (face stage)");
         int optin = 0;
         HF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "cudaDeviceGetAttribute");
         d.smem_optin = (size_t)optin;
@@ -518,9 +520,12 @@ int hf_particle_update(const hf_plan* p, void* stream) {
 int hf_face_stage(const hf_plan* p, double dt, void* stream) {
     int rc = check_plan(p);
     if (rc) return rc;
-    if (!p->num_chunks) return HF_OK;
-    hf::k_face_stage<<<p->num_chunks * hf::kStageSplit, hf::kThreads, 0, S(stream)>>>(static_cast<const hf_scene*>(p->scenes_dev),
-                                                                   static_cast<const hf::WorkItem*>(p->work_dev), dt);
+    if (!p->num_tiles) return HF_OK;
+    DeviceInfo* d = nullptr;
+    if ((rc = device_info(&d))) return rc;
+    // one 512-thread block per CG tile, the old velocities around the tile staged in shared memory
+    hf::k_face_tile<<<p->num_tiles, 512, hf::face_tile_smem(), S(stream)>>>(static_cast<const hf_scene*>(p->scenes_dev),
+                                                                        static_cast<const hf::TileItem*>(p->tiles_dev), dt);
     HF_CUDA(cudaGetLastError(), "launch (face stage)");
     return HF_OK;
 }

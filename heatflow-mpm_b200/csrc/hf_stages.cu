@@ -428,11 +428,123 @@ __device__ __forceinline__ float relax_face(float q, float af, float kf, float m
     return __fdiv_rn(__fadd_rn(q, __fmul_rn(dtc, mf)), __fadd_rn(1.0f, __fmul_rn(dtc, kf)));
 }
 
-__global__ void __launch_bounds__(kThreads, 4) k_face_stage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
-                                                        double dt_d) {
-    const WorkItem wi = work[blockIdx.x / kStageSplit];
-    const hf_scene& S = scenes[wi.scene];
-    const int n = S.n, N = n * n * n;
+// ------------------------------------------------------------------- face stage from staged velocity boxes
+// The face stage per CG tile (4 x 8 x 32 cells, 512 threads, two cells per thread): the old u, v, w around the tile are
+// staged in shared memory as boxes with a kFH-cell halo whose entries outside the lattice repeat the nearest lattice
+// node.  A trilinear sample whose eight nodes fall in the box then reads box[lower - origin] and its +1 neighbours,
+// which hold lattice[clamp(lower)] and lattice[clamp(lower + 1)] -- exactly the nodes fields.py:16-28 reads after
+// clamping -- with 32-bit shared addresses and no clamps; a sample outside the box (a back-trace longer than the halo)
+// reads the lattice itself.  Positions, weights and the order of every operation are those of sample_axes, so the
+// results are the same bits as sampling the lattice directly (fields.py's clamped nodes).
+constexpr int kFH = 2;
+constexpr int kFBX = kTI + 2 * kFH + 1, kFBY = kTJ + 2 * kFH + 1, kFBZ = kTK + 2 * kFH + 1;   // 9 x 13 x 37
+constexpr int kFBox = kFBX * kFBY * kFBZ;
+constexpr int kFaceThreads = 512;
+constexpr size_t kFaceSmem = 3 * (size_t)kFBox * sizeof(float);
+
+// one axis of a sample: unclamped lower node i (box-local: i - origin), weights w0 = 1 - f and f (fields.py:14-27)
+struct BAxis {
+    int i, b;
+    float w0, f;
+};
+
+__device__ __forceinline__ BAxis baxis(float q, float off, int origin) {
+    const float g = __fsub_rn(q, off);
+    const int i = (int)floorf(g);
+    const float f = __fsub_rn(g, (float)i);
+    return BAxis{i, i - origin, __fsub_rn(1.0f, f), f};
+}
+
+__device__ __forceinline__ bool in_box(const BAxis& X, const BAxis& Y, const BAxis& Z) {
+    return (unsigned)X.b <= (unsigned)(kFBX - 2) && (unsigned)Y.b <= (unsigned)(kFBY - 2) &&
+           (unsigned)Z.b <= (unsigned)(kFBZ - 2);
+}
+
+// sample_axes' eight terms in its order, from a box or (outside it) from the lattice with the clamped nodes
+__device__ __forceinline__ float box_sample(const float* __restrict__ B, const float* __restrict__ a, const BAxis& X,
+                                            const BAxis& Y, const BAxis& Z, int nx, int ny, int nz) {
+    float v[8];
+    if (in_box(X, Y, Z)) {
+        const float* c = B + (X.b * kFBY + Y.b) * kFBZ + Z.b;
+        v[0] = c[0];
+        v[1] = c[1];
+        v[2] = c[kFBZ];
+        v[3] = c[kFBZ + 1];
+        v[4] = c[kFBY * kFBZ];
+        v[5] = c[kFBY * kFBZ + 1];
+        v[6] = c[kFBY * kFBZ + kFBZ];
+        v[7] = c[kFBY * kFBZ + kFBZ + 1];
+    } else {
+        const int x0 = clampi(X.i, 0, nx - 1), x1 = clampi(X.i + 1, 0, nx - 1);
+        const int y0 = clampi(Y.i, 0, ny - 1), y1 = clampi(Y.i + 1, 0, ny - 1);
+        const int z0 = clampi(Z.i, 0, nz - 1), z1 = clampi(Z.i + 1, 0, nz - 1);
+        const int sy = nz, sx = ny * nz;
+        v[0] = __ldg(a + x0 * sx + y0 * sy + z0);
+        v[1] = __ldg(a + x0 * sx + y0 * sy + z1);
+        v[2] = __ldg(a + x0 * sx + y1 * sy + z0);
+        v[3] = __ldg(a + x0 * sx + y1 * sy + z1);
+        v[4] = __ldg(a + x1 * sx + y0 * sy + z0);
+        v[5] = __ldg(a + x1 * sx + y0 * sy + z1);
+        v[6] = __ldg(a + x1 * sx + y1 * sy + z0);
+        v[7] = __ldg(a + x1 * sx + y1 * sy + z1);
+    }
+    float s = 0.0f;
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.w0), Z.w0), v[0]));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.w0), Z.f), v[1]));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.f), Z.w0), v[2]));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.f), Z.f), v[3]));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.w0), Z.w0), v[4]));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.w0), Z.f), v[5]));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.f), Z.w0), v[6]));
+    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.f), Z.f), v[7]));
+    return s;
+}
+
+// sample_velocity (fields.py:68-72) from the boxes: the three lattices at one point
+__device__ __forceinline__ void box_velocity(const float* Bu, const float* Bv, const float* Bw, const float* __restrict__ u,
+                                             const float* __restrict__ v, const float* __restrict__ w, float px,
+                                             float py, float pz, const DivBy& h, int n, int ox, int oy, int oz, float* o) {
+    const GridPos q = grid_pos(px, py, pz, h);
+    const BAxis x0 = baxis(q.x, 0.0f, ox), x5 = baxis(q.x, 0.5f, ox);
+    const BAxis y0 = baxis(q.y, 0.0f, oy), y5 = baxis(q.y, 0.5f, oy);
+    const BAxis z0 = baxis(q.z, 0.0f, oz), z5 = baxis(q.z, 0.5f, oz);
+    o[0] = box_sample(Bu, u, x0, y5, z5, n + 1, n, n);
+    o[1] = box_sample(Bv, v, x5, y0, z5, n, n + 1, n);
+    o[2] = box_sample(Bw, w, x5, y5, z0, n, n, n + 1);
+}
+
+// backtrace (fields.py:111-116) from the boxes
+__device__ __forceinline__ void box_backtrace(const float* Bu, const float* Bv, const float* Bw, const float* __restrict__ u,
+                                              const float* __restrict__ v, const float* __restrict__ w, const float* x,
+                                              const DivBy& h, int n, float dt, int ox, int oy, int oz, float* o) {
+    float vel[3];
+    box_velocity(Bu, Bv, Bw, u, v, w, x[0], x[1], x[2], h, n, ox, oy, oz, vel);
+    const float hdt = __fmul_rn(0.5f, dt);
+    const float y0 = __fsub_rn(x[0], __fmul_rn(hdt, vel[0]));
+    const float y1 = __fsub_rn(x[1], __fmul_rn(hdt, vel[1]));
+    const float y2 = __fsub_rn(x[2], __fmul_rn(hdt, vel[2]));
+    box_velocity(Bu, Bv, Bw, u, v, w, y0, y1, y2, h, n, ox, oy, oz, vel);
+    o[0] = __fsub_rn(x[0], __fmul_rn(dt, vel[0]));
+    o[1] = __fsub_rn(x[1], __fmul_rn(dt, vel[1]));
+    o[2] = __fsub_rn(x[2], __fmul_rn(dt, vel[2]));
+}
+
+// sample (fields.py:5-36) of one lattice with offsets (offx, offy, offz) from its box
+__device__ __forceinline__ float box_point(const float* B, const float* __restrict__ a, const float* y, float offx,
+                                           float offy, float offz, const DivBy& h, int nx, int ny, int nz, int ox, int oy,
+                                           int oz) {
+    const GridPos q = grid_pos(y[0], y[1], y[2], h);
+    return box_sample(B, a, baxis(q.x, offx, ox), baxis(q.y, offy, oy), baxis(q.z, offz, oz), nx, ny, nz);
+}
+
+// grid.py:219-233 for the faces of the cells of one CG tile (relax_face's fused per-face arithmetic, sampling from the
+// staged boxes); block = 512 threads, thread lt owns cells (i0 + 2 (lt / 256) + {0, 1}, j0 + (lt % 256) / 32, k0 + lt % 32).
+__global__ void __launch_bounds__(kFaceThreads, 2) k_face_tile(const hf_scene* __restrict__ scenes,
+                                                              const TileItem* __restrict__ tiles, double dt_d) {
+    extern __shared__ float fbox[];
+    const TileItem ti = tiles[blockIdx.x];
+    const hf_scene& S = scenes[ti.scene];
+    const int n = S.n;
     const int par = S.state->parity;
     const float *u0 = S.u[par], *v0 = S.v[par], *w0 = S.w[par];
     float *u1 = S.u[par ^ 1], *v1 = S.v[par ^ 1], *w1 = S.w[par ^ 1];
@@ -442,12 +554,29 @@ __global__ void __launch_bounds__(kThreads, 4) k_face_stage(const hf_scene* __re
     const bool buoy = (S.flags & HF_FLAG_BUOYANCY) != 0;
     const float buoy_num = __fmul_rn(dt, g);
     const DivBy hd = div_by(h), buoy_den = div_by(__fadd_rn(t_amb, 273.15f));
-    const int m0 = (int)(blockIdx.x % kStageSplit) * (kCellsPerThread / kStageSplit);
-    for (int m = m0; m < m0 + kCellsPerThread / kStageSplit; ++m) {
-        const int t = wi.first + threadIdx.x + m * kThreads;
-        if (t >= N) break;
-        int i, j, k;
-        cell_ijk(t, n, i, j, k);
+    float* Bu = fbox;
+    float* Bv = fbox + kFBox;
+    float* Bw = fbox + 2 * kFBox;
+    const int ox = ti.i0 - kFH, oy = ti.j0 - kFH, oz = ti.k0 - kFH;
+    // the boxes: lattice node (ox + a, oy + b, oz + c), clamped to the lattice
+    for (int e = threadIdx.x; e < kFBox; e += kFaceThreads) {
+        const int a = e / (kFBY * kFBZ), r = e - a * (kFBY * kFBZ), b = r / kFBZ, c = r - b * kFBZ;
+        const int gi = ox + a, gj = oy + b, gk = oz + c;
+        const int iu = clampi(gi, 0, n), ic = clampi(gi, 0, n - 1);
+        const int ju = clampi(gj, 0, n), jc = clampi(gj, 0, n - 1);
+        const int ku = clampi(gk, 0, n), kc = clampi(gk, 0, n - 1);
+        Bu[e] = __ldg(u0 + (iu * n + jc) * n + kc);               // (n+1, n, n)
+        Bv[e] = __ldg(v0 + (ic * (n + 1) + ju) * n + kc);         // (n, n+1, n)
+        Bw[e] = __ldg(w0 + (ic * n + jc) * (n + 1) + ku);         // (n, n, n+1)
+    }
+    __syncthreads();
+    const int lt = threadIdx.x & 255;
+    const int j = ti.j0 + (lt >> 5), k = ti.k0 + (lt & 31);
+    if (j >= n || k >= n) return;
+    for (int mm = 0; mm < 2; ++mm) {
+        const int i = ti.i0 + 2 * (threadIdx.x >> 8) + mm;
+        if (i >= n) break;
+        const int t = (i * n + j) * n + k;
         const float fi = (float)i, fj = (float)j, fk = (float)k;
         const float ci = __fmul_rn(__fadd_rn(fi, 0.5f), h), cj = __fmul_rn(__fadd_rn(fj, 0.5f), h),
                     ck = __fmul_rn(__fadd_rn(fk, 0.5f), h);
@@ -458,8 +587,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_face_stage(const hf_scene* __re
             float val = 0.0f;
             if (i != 0) {
                 const float x[3] = {__fmul_rn(fi, h), cj, ck};
-                backtrace(u0, v0, w0, x, hd, n, dt, y);
-                val = sample(u0, y[0], y[1], y[2], 0.0f, 0.5f, 0.5f, hd, n + 1, n, n);
+                box_backtrace(Bu, Bv, Bw, u0, v0, w0, x, hd, n, dt, ox, oy, oz, y);
+                val = box_point(Bu, u0, y, 0.0f, 0.5f, 0.5f, hd, n + 1, n, n, ox, oy, oz);
                 val = relax_face(val, S.ax[f], S.kx[f], S.mx[f], rho, afmin, h, dt);
             }
             u1[f] = val;
@@ -471,8 +600,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_face_stage(const hf_scene* __re
             float val = 0.0f;
             if (j != 0) {
                 const float x[3] = {ci, __fmul_rn(fj, h), ck};
-                backtrace(u0, v0, w0, x, hd, n, dt, y);
-                val = sample(v0, y[0], y[1], y[2], 0.5f, 0.0f, 0.5f, hd, n, n + 1, n);
+                box_backtrace(Bu, Bv, Bw, u0, v0, w0, x, hd, n, dt, ox, oy, oz, y);
+                val = box_point(Bv, v0, y, 0.5f, 0.0f, 0.5f, hd, n, n + 1, n, ox, oy, oz);
                 val = relax_face(val, S.ay[f], S.ky[f], S.my[f], rho, afmin, h, dt);
             }
             v1[f] = val;
@@ -484,8 +613,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_face_stage(const hf_scene* __re
             float val = 0.0f;
             if (k != 0) {
                 const float x[3] = {ci, cj, __fmul_rn(fk, h)};
-                backtrace(u0, v0, w0, x, hd, n, dt, y);
-                val = sample(w0, y[0], y[1], y[2], 0.5f, 0.5f, 0.0f, hd, n, n, n + 1);
+                box_backtrace(Bu, Bv, Bw, u0, v0, w0, x, hd, n, dt, ox, oy, oz, y);
+                val = box_point(Bw, w0, y, 0.5f, 0.5f, 0.0f, hd, n, n, n + 1, ox, oy, oz);
                 if (buoy) {
                     const float tf = __fmul_rn(0.5f, __fadd_rn(Tn[t - 1], Tn[t]));
                     val = __fadd_rn(val, div_rn(__fmul_rn(buoy_num, __fsub_rn(tf, t_amb)), buoy_den));
@@ -497,6 +626,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_face_stage(const hf_scene* __re
         }
     }
 }
+
+size_t face_tile_smem() { return kFaceSmem; }
 
 // grid.py:82-91 k_divergence_rhs with scale rho/dt into rhs, plus the fp64 partial sum of the chunk for the mean of
 // grid.py:238-241 (reduced over the scene by the pressure CG kernel, in a fixed tree).

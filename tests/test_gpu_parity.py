@@ -303,17 +303,21 @@ def test_divide_by_constant_matches_ieee(torch_cuda):
         check(torch.tensor([0, -2 ** 31, 1, 0x7F800000, -8388608, 0x7FC00000], dtype=torch.int32, device="cuda"))
 
 
-def test_sampling_stages_bit_exact_vs_oracle(torch_cuda):
+@pytest.mark.parametrize("n,vmax", [(20, 3.0), (20, 40.0), (40, 6.0)])
+def test_sampling_stages_bit_exact_vs_oracle(torch_cuda, n, vmax):
     """The face stage (semi-Lagrangian advection of u, v, w + buoyancy + relaxation, grid.py:25-79) and the temperature
     stage's advection (heat.py:21-41 with the blend, fixed cells and source) against the oracle's kernels, bit for bit
-    (compared as integers), on a random air-only scene whose velocities carry back-traces outside the domain."""
+    (compared as integers), on a random air-only scene whose velocities carry back-traces outside the domain.  The
+    face stage samples from velocity boxes staged around each tile with a two-cell halo: |u| dt / h is 0.25 cells at
+    (20, 3 m/s), so every back-trace stays in the boxes; 3.3 cells at (20, 40 m/s), so most leave them and read the
+    lattice; up to 1 cell at (40, 6 m/s), a mix."""
     torch = torch_cuda
     from heatflow_mpm.scene import DeviceScene, ScenePlan
     from oracle.oracle import Kernels
-    n, dt = 20, 2e-3
+    dt = 2e-3
     spec, T0, uvw = random_scene_inputs(n, seed=9)
     rng = np.random.default_rng(4)
-    uvw = [rng.uniform(-3.0, 3.0, a.shape).astype(np.float32) for a in uvw]
+    uvw = [rng.uniform(-vmax, vmax, a.shape).astype(np.float32) for a in uvw]
     sc = DeviceScene(spec)
     plan = ScenePlan([sc])
     plan.prepare_statics()
