@@ -75,6 +75,9 @@ int device_info(DeviceInfo** out) {
                 "occupancy");
         HF_CUDA(cudaFuncSetAttribute(hf::k_face_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hf::face_tile_smem()),
                 "smem attribute (face stage)");
+        HF_CUDA(cudaFuncSetAttribute(hf::k_advect_T_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)hf::advect_tile_smem()),
+                "smem attribute (temperature stage)");
         int optin = 0;
         HF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "cudaDeviceGetAttribute");
         d.smem_optin = (size_t)optin;
@@ -492,8 +495,12 @@ int hf_temperature_stage(const hf_plan* p, double dt, void* stream) {
     if (!p->num_chunks) return HF_OK;
     const hf_scene* scenes = static_cast<const hf_scene*>(p->scenes_dev);
     const hf::WorkItem* work = static_cast<const hf::WorkItem*>(p->work_dev);
+    DeviceInfo* d = nullptr;
+    if ((rc = device_info(&d))) return rc;
     hf::k_prestage<<<p->num_chunks, hf::kThreads, 0, S(stream)>>>(scenes, work, dt);
-    hf::k_advect_T<<<p->num_chunks * hf::kStageSplit, hf::kThreads, 0, S(stream)>>>(scenes, work, dt);
+    // one 512-thread block per CG tile, the old velocities and Tw around the tile staged in shared memory
+    hf::k_advect_T_tile<<<p->num_tiles, 512, hf::advect_tile_smem(), S(stream)>>>(
+        scenes, static_cast<const hf::TileItem*>(p->tiles_dev), dt);
     HF_CUDA(cudaGetLastError(), "launch (temperature stage)");
     return HF_OK;
 }

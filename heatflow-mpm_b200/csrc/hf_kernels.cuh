@@ -50,10 +50,11 @@ __global__ void k_coeff(const hf_scene* __restrict__ scenes, const WorkItem* __r
 __global__ void k_obstacle_box(const hf_scene* __restrict__ scenes, int s);
 __global__ void k_coeff_box(const hf_scene* __restrict__ scenes, int s);
 __global__ void k_prestage(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt);
-__global__ void k_advect_T(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt);
 __global__ void k_particle_update(const hf_scene* __restrict__ scenes, int s);
 __global__ void k_face_tile(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, double dt);
 size_t face_tile_smem();   // dynamic shared memory of k_face_tile (512-thread blocks)
+__global__ void k_advect_T_tile(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, double dt);
+size_t advect_tile_smem();   // dynamic shared memory of k_advect_T_tile (512-thread blocks)
 __global__ void k_divergence(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, double dt, Workspace ws);
 __global__ void k_cell_velocity(const hf_scene* __restrict__ scenes, int s, float* __restrict__ out);
 __global__ void k_divergence_max(const hf_scene* __restrict__ scenes, int s, unsigned* __restrict__ out_bits);

@@ -321,69 +321,6 @@ __global__ void __launch_bounds__(kThreads) k_prestage(const hf_scene* __restric
     }
 }
 
-// solver.py:78 k_advect (heat.py:31-41) into T[parity^1], fused with k_heat_rhs (heat.py:108-118) which only needs
-// the advected value of the same cell.
-__global__ void __launch_bounds__(kThreads, 4) k_advect_T(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
-                                                      double dt_d) {
-    const WorkItem wi = work[blockIdx.x / kStageSplit];
-    const hf_scene& S = scenes[wi.scene];
-    const int n = S.n, N = n * n * n;
-    const int par = S.state->parity;
-    const float *u = S.u[par], *v = S.v[par], *w = S.w[par];
-    float* T2 = S.T[par ^ 1];
-    const float h = (float)S.h, dt = (float)dt_d;
-    const float* Tw = S.Tw;
-    const uint8_t* fl = S.cell_flags;
-    const float c_dt = __fdiv_rn(dt, __fmul_rn(h, h));
-    const DivBy hd = div_by(h);
-    const int m0 = (int)(blockIdx.x % kStageSplit) * (kCellsPerThread / kStageSplit);
-    for (int m = m0; m < m0 + kCellsPerThread / kStageSplit; ++m) {
-        const int t = wi.first + threadIdx.x + m * kThreads;
-        if (t >= N) break;
-        int i, j, k;
-        cell_ijk(t, n, i, j, k);
-        // the heat rhs's flags and face diffusivities are loaded first (in bounds: a missing neighbour reads the cell
-        // itself, the face lattices have n + 1 layers), so they arrive while the back-trace is computed
-        const int nbr[6] = {t - n * n, t + n * n, t - n, t + n, t - 1, t + 1};
-        const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
-        const uint8_t fc = fl[t];
-        uint8_t fn[6];
-        float kf[6];
-        const float* hk[6] = {S.hkx + uidx(n, i, j, k), S.hkx + uidx(n, i + 1, j, k), S.hky + vidx(n, i, j, k),
-                              S.hky + vidx(n, i, j + 1, k), S.hkz + widx(n, i, j, k), S.hkz + widx(n, i, j, k + 1)};
-#pragma unroll
-        for (int s = 0; s < 6; ++s) {
-            fn[s] = fl[in[s] ? nbr[s] : t];
-            kf[s] = *hk[s];
-        }
-        float out;
-        if (S.alpha_s[t] > 0.5f) {
-            out = Tw[t];
-        } else {
-            float x[3] = {__fmul_rn(__fadd_rn((float)i, 0.5f), h), __fmul_rn(__fadd_rn((float)j, 0.5f), h),
-                          __fmul_rn(__fadd_rn((float)k, 0.5f), h)};
-            float y[3];
-            backtrace(u, v, w, x, hd, n, dt, y);
-            out = sample(Tw, y[0], y[1], y[2], 0.5f, 0.5f, 0.5f, hd, n, n, n);
-        }
-        T2[t] = out;
-        // heat rhs: tfix on fixed cells, else T2 + dt/h^2 * sum over fixed neighbours of kappa_f * tfix
-        float rhs;
-        if (fc & 1) {
-            rhs = S.tfix[t];
-        } else {
-            float acc = 0.0f;
-#pragma unroll
-            for (int s = 0; s < 6; ++s) {
-                if (!in[s]) continue;
-                if (fn[s] & 1) acc = __fadd_rn(acc, __fmul_rn(kf[s], S.tfix[nbr[s]]));
-            }
-            rhs = __fadd_rn(out, __fmul_rn(c_dt, acc));
-        }
-        S.hrhs[t] = rhs;
-    }
-}
-
 // heat.py:161-174 k_particle_update: FLIP increment between Tw and the diffused T, melt law
 __global__ void __launch_bounds__(kThreads) k_particle_update(const hf_scene* __restrict__ scenes, int s) {
     const hf_scene& S = scenes[s];
@@ -628,6 +565,91 @@ __global__ void __launch_bounds__(kFaceThreads, 2) k_face_tile(const hf_scene* _
 }
 
 size_t face_tile_smem() { return kFaceSmem; }
+
+// solver.py:78 k_advect (heat.py:31-41) into T[parity^1], fused with k_heat_rhs (heat.py:108-118), per CG tile: the
+// old u, v, w and Tw around the tile staged in shared memory as in k_face_tile (the same bits as sampling the
+// lattices directly).  512 threads, two cells per thread.
+__global__ void __launch_bounds__(kFaceThreads, 2) k_advect_T_tile(const hf_scene* __restrict__ scenes,
+                                                                  const TileItem* __restrict__ tiles, double dt_d) {
+    extern __shared__ float fbox[];
+    const TileItem ti = tiles[blockIdx.x];
+    const hf_scene& S = scenes[ti.scene];
+    const int n = S.n;
+    const int par = S.state->parity;
+    const float *u = S.u[par], *v = S.v[par], *w = S.w[par];
+    float* T2 = S.T[par ^ 1];
+    const float h = (float)S.h, dt = (float)dt_d;
+    const float* Tw = S.Tw;
+    const uint8_t* fl = S.cell_flags;
+    const float c_dt = __fdiv_rn(dt, __fmul_rn(h, h));
+    const DivBy hd = div_by(h);
+    float* Bu = fbox;
+    float* Bv = fbox + kFBox;
+    float* Bw = fbox + 2 * kFBox;
+    float* BT = fbox + 3 * kFBox;
+    const int ox = ti.i0 - kFH, oy = ti.j0 - kFH, oz = ti.k0 - kFH;
+    for (int e = threadIdx.x; e < kFBox; e += kFaceThreads) {
+        const int a = e / (kFBY * kFBZ), r = e - a * (kFBY * kFBZ), b = r / kFBZ, c = r - b * kFBZ;
+        const int gi = ox + a, gj = oy + b, gk = oz + c;
+        const int iu = clampi(gi, 0, n), ic = clampi(gi, 0, n - 1);
+        const int ju = clampi(gj, 0, n), jc = clampi(gj, 0, n - 1);
+        const int ku = clampi(gk, 0, n), kc = clampi(gk, 0, n - 1);
+        Bu[e] = __ldg(u + (iu * n + jc) * n + kc);                // (n+1, n, n)
+        Bv[e] = __ldg(v + (ic * (n + 1) + ju) * n + kc);          // (n, n+1, n)
+        Bw[e] = __ldg(w + (ic * n + jc) * (n + 1) + ku);          // (n, n, n+1)
+        BT[e] = __ldg(Tw + (ic * n + jc) * n + kc);               // (n, n, n)
+    }
+    __syncthreads();
+    const int lt = threadIdx.x & 255;
+    const int j = ti.j0 + (lt >> 5), k = ti.k0 + (lt & 31);
+    if (j >= n || k >= n) return;
+    for (int mm = 0; mm < 2; ++mm) {
+        const int i = ti.i0 + 2 * (threadIdx.x >> 8) + mm;
+        if (i >= n) break;
+        const int t = (i * n + j) * n + k;
+        // the heat rhs's flags and face diffusivities are loaded first (in bounds: a missing neighbour reads the cell
+        // itself, the face lattices have n + 1 layers), so they arrive while the back-trace is computed
+        const int nbr[6] = {t - n * n, t + n * n, t - n, t + n, t - 1, t + 1};
+        const bool in[6] = {i > 0, i < n - 1, j > 0, j < n - 1, k > 0, k < n - 1};
+        const uint8_t fc = fl[t];
+        uint8_t fn[6];
+        float kf[6];
+        const float* hk[6] = {S.hkx + uidx(n, i, j, k), S.hkx + uidx(n, i + 1, j, k), S.hky + vidx(n, i, j, k),
+                              S.hky + vidx(n, i, j + 1, k), S.hkz + widx(n, i, j, k), S.hkz + widx(n, i, j, k + 1)};
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            fn[s] = fl[in[s] ? nbr[s] : t];
+            kf[s] = *hk[s];
+        }
+        float out;
+        if (S.alpha_s[t] > 0.5f) {
+            out = Tw[t];
+        } else {
+            const float x[3] = {__fmul_rn(__fadd_rn((float)i, 0.5f), h), __fmul_rn(__fadd_rn((float)j, 0.5f), h),
+                                __fmul_rn(__fadd_rn((float)k, 0.5f), h)};
+            float y[3];
+            box_backtrace(Bu, Bv, Bw, u, v, w, x, hd, n, dt, ox, oy, oz, y);
+            out = box_point(BT, Tw, y, 0.5f, 0.5f, 0.5f, hd, n, n, n, ox, oy, oz);
+        }
+        T2[t] = out;
+        // heat rhs: tfix on fixed cells, else T2 + dt/h^2 * sum over fixed neighbours of kappa_f * tfix
+        float rhs;
+        if (fc & 1) {
+            rhs = S.tfix[t];
+        } else {
+            float acc = 0.0f;
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                if (!in[s]) continue;
+                if (fn[s] & 1) acc = __fadd_rn(acc, __fmul_rn(kf[s], S.tfix[nbr[s]]));
+            }
+            rhs = __fadd_rn(out, __fmul_rn(c_dt, acc));
+        }
+        S.hrhs[t] = rhs;
+    }
+}
+
+size_t advect_tile_smem() { return 4 * (size_t)kFBox * sizeof(float); }
 
 // grid.py:82-91 k_divergence_rhs with scale rho/dt into rhs, plus the fp64 partial sum of the chunk for the mean of
 // grid.py:238-241 (reduced over the scene by the pressure CG kernel, in a fixed tree).
