@@ -434,8 +434,8 @@ def bench_plain(args, dev, rank, world, local):
     h_iters = int(st1.total_heat_iters - st0.total_heat_iters)
     cg_ms = sum(a.elapsed_time(b) for a, b in pe)
     value = world * steps / (el_ms / 1000.0)
-    # footprint, scatter, obstacle, coeff, prestage, advect_T, heat CG, particle update, face, divergence, pressure CG
-    launches_per_step = 11
+    # scatter (+ footprint box), obstacle, coeff, prestage, advect_T, heat CG, particle update, face, divergence, pressure CG
+    launches_per_step = 10
     stage_ms = stage_breakdown(plan, [("obstacle", plan.obstacle_fields), ("temperature", lambda: plan.temperature_stage(DT)),
                                       ("heat_cg", lambda: plan.heat_solve(DT)), ("particles", plan.particle_update),
                                       ("face", lambda: plan.face_stage(DT)), ("divergence", lambda: plan.divergence_stage(DT)),

@@ -466,7 +466,6 @@ int hf_obstacle_fields(const hf_plan* p, int all_scenes, void* stream) {
         const hf_scene& sc = p->scenes_host[s];
         if (!(sc.flags & HF_FLAG_ACTIVE) || !(sc.flags & HF_FLAG_PARTICLES) || sc.n_particles <= 0) continue;
         if (!sc.acc || !sc.pos || !sc.pvel || !sc.ptemp) return fail(HF_ERR_ARG, "coupled scene without particle buffers");
-        hf::k_footprint<<<(sc.n_particles + hf::kThreads - 1) / hf::kThreads, hf::kThreads, 0, S(stream)>>>(scenes, s);
         hf::k_scatter<<<(sc.n_particles + hf::kThreads - 1) / hf::kThreads, hf::kThreads, 0, S(stream)>>>(scenes, s);
     }
     if (!all_scenes) {

@@ -43,7 +43,6 @@ struct TileMaps {
 };
 
 __global__ void k_scatter(const hf_scene* __restrict__ scenes, int s);
-__global__ void k_footprint(const hf_scene* __restrict__ scenes, int s);
 __global__ void k_obstacle(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, int all_scenes);
 __global__ void k_coeff(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work, int all_scenes);
 // the per-substep rebuild of one coupled scene, over its footprint boxes only

@@ -48,12 +48,42 @@ __device__ __forceinline__ void scatter_fx(long long* acc, float px, float py, f
     }
 }
 
+// Cells whose obstacle fields a particle can touch: floor(x/h) - 1 .. floor(x/h) + 1 per axis covers the cell lattice
+// (offset 1/2) and the face lattices (offset 0 or 1/2), the high wall face included (it belongs to cell n-1).
+__device__ __forceinline__ void footprint(float x, float h, int n, int& lo, int& hi) {
+    const int c = (int)floorf(__fdiv_rn(x, h));
+    lo = clampi(c - 1, 0, n - 1);
+    hi = clampi(c + 1, 0, n - 1);
+}
+
+// One launch per substep for the particles' two passes: the footprint box of this substep (the cells whose obstacle
+// fields a particle can touch, a min/max over particles) and the fixed-point scatter of solver.py:19-38 / heat.py:12-18.
 __global__ void __launch_bounds__(kThreads) k_scatter(const hf_scene* __restrict__ scenes, int s) {
     const hf_scene& S = scenes[s];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= S.n_particles) return;
     const int n = S.n;
-    const float h = (float)S.h, vol = (float)S.vol, k0 = (float)S.k_particle;
+    const float h = (float)S.h;
+    {
+        int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+        if (t < S.n_particles) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) footprint(S.pos[3 * t + d], h, n, lo[d], hi[d]);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
+            hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
+        }
+        if ((threadIdx.x & 31) == 0 && lo[0] <= hi[0]) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                atomicMin(&S.state->box[d], lo[d]);
+                atomicMax(&S.state->box[3 + d], hi[d]);
+            }
+        }
+    }
+    if (t >= S.n_particles) return;
+    const float vol = (float)S.vol, k0 = (float)S.k_particle;
     const long long M = (long long)(n + 1) * (n + 1) * (n + 1);
     long long* acc = S.acc;
     const float px = S.pos[3 * t], py = S.pos[3 * t + 1], pz = S.pos[3 * t + 2];
@@ -71,38 +101,6 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const hf_scene* __restrict
     scatter_fx(acc + 9 * M, px, py, pz, 0.5f, 0.5f, 0.0f, h, n, n, n + 1, __fmul_rn(k0, vz));
     scatter_fx(acc + 10 * M, px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n, frac);
     scatter_fx(acc + 11 * M, px, py, pz, 0.5f, 0.5f, 0.5f, h, n, n, n, __fmul_rn(frac, S.ptemp[t]));
-}
-
-// Cells whose obstacle fields a particle can touch: floor(x/h) - 1 .. floor(x/h) + 1 per axis covers the cell lattice
-// (offset 1/2) and the face lattices (offset 0 or 1/2), the high wall face included (it belongs to cell n-1).
-__device__ __forceinline__ void footprint(float x, float h, int n, int& lo, int& hi) {
-    const int c = (int)floorf(__fdiv_rn(x, h));
-    lo = clampi(c - 1, 0, n - 1);
-    hi = clampi(c + 1, 0, n - 1);
-}
-
-__global__ void __launch_bounds__(kThreads) k_footprint(const hf_scene* __restrict__ scenes, int s) {
-    const hf_scene& S = scenes[s];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n = S.n;
-    const float h = (float)S.h;
-    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
-    if (t < S.n_particles) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) footprint(S.pos[3 * t + d], h, n, lo[d], hi[d]);
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
-        hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
-    }
-    if ((threadIdx.x & 31) == 0 && lo[0] <= hi[0]) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            atomicMin(&S.state->box[d], lo[d]);
-            atomicMax(&S.state->box[3 + d], hi[d]);
-        }
-    }
 }
 
 __device__ __forceinline__ bool in_box(const int* b, int i, int j, int k, int grow_hi) {
