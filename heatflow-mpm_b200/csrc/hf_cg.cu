@@ -123,6 +123,61 @@ __device__ __forceinline__ void scene_sums(const double* __restrict__ buf, int b
     }
 }
 
+// scene_sums for every live scene q < ns of a group (scene scene_lo + q: items tile_begin[s] .. tile_begin[s + 1]), with
+// the same tree per scene, in passes of kRedComps * 32 / (8 K) scenes that share one pair of block barriers instead of
+// a pair per scene; fn(q, tot) then runs once per live scene, in one thread, with the scene's K sums.  live(q) must
+// not change before fn runs for q.  256-thread blocks.
+template <int K, class Live, class Fn>
+__device__ __forceinline__ void group_sums(const double* __restrict__ buf, const int* __restrict__ tile_begin,
+                                           int scene_lo, int ns, const int (&comp)[K], int cs, double* red, Live live,
+                                           Fn fn) {
+    constexpr int CH = kRedComps * 32 / (8 * K);
+    const int lt = threadIdx.x, lane = lt & 31, warp = lt >> 5;
+    for (int q0 = 0; q0 < ns; q0 += CH) {
+        const int qn = ns - q0 < CH ? ns - q0 : CH;
+        for (int qq = 0; qq < qn; ++qq) {
+            if (!live(q0 + qq)) continue;
+            const int b = tile_begin[scene_lo + q0 + qq], e = tile_begin[scene_lo + q0 + qq + 1];
+            double acc[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] = 0.0;
+            for (int c = b + lt; c < e; c += 4 * kThreads) {
+                double v[4][K];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int k = 0; k < K; ++k) v[u][k] = c + u * kThreads < e ? buf[comp[k] * cs + c + u * kThreads] : 0.0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int k = 0; k < K; ++k) acc[k] += v[u][k];
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) red[(qq * K + k) * 8 + warp] = acc[k];
+            }
+        }
+        __syncthreads();
+        if (lt < qn && live(q0 + lt)) {
+            double tot[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                double t = 0.0;
+#pragma unroll
+                for (int w = 0; w < kThreads / 32; ++w) t += red[(lt * K + k) * 8 + w];
+                tot[k] = t;
+            }
+            fn(q0 + lt, tot);
+        }
+        __syncthreads();
+    }
+}
+
 // Per-256-thread-group sum (each group reduces its own 8 warps in index order): the tile partial tree.
 template <int K>
 __device__ __forceinline__ void group_sum(double (&v)[K], double* red) {
@@ -843,18 +898,15 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             if (lt == 0) bufA[c] = part[0];
         }
         if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
-        for (int q = 0; q < ns; ++q) {
-            if (!loc[q].live) continue;   // uniform: shared value written before the last __syncthreads
-            const int s = scene_lo + q;
-            double tot[1];
+        {
+            // every live scene's p.Ap (live: shared values written before the last __syncthreads)
             const int comp[1] = {0};
-            scene_sums<1>(bufA, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red, ws.tiles);
-            if (threadIdx.x == 0) {
-                loc[q].pAp = tot[0];
-                loc[q].alpha = __double2float_rn(loc[q].rz / tot[0]);
-            }
+            group_sums<1>(bufA, ws.tile_begin, scene_lo, ns, comp, ws.tiles, red, [&](int q) { return (bool)loc[q].live; },
+                          [&](int q, const double(&tot)[1]) {
+                              loc[q].pAp = tot[0];
+                              loc[q].alpha = __double2float_rn(loc[q].rz / tot[0]);
+                          });
         }
-        __syncthreads();
         // phase B: x += alpha p, r -= alpha Ap, z = D r, r.r and r.z
         if constexpr (TMA) {
             // the tile's x, p_k, r, Ap and D as five (32, 8, 4) boxes: element (m, lt / 32, lt % 32) at m 256 + lt
@@ -942,13 +994,11 @@ __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem*
             }
         }
         if (!(ok = grid_barrier(bar, epoch, ws.err, nlb))) goto done;
-        for (int q = 0; q < ns; ++q) {
-            if (!loc[q].live) continue;
-            const int s = scene_lo + q;
-            double tot[2];
+        {
+            // every live scene's r.r and r.z, then its convergence test
             const int comp[2] = {1, 2};
-            scene_sums<2>(bufB, ws.tile_begin[s], ws.tile_begin[s + 1], comp, tot, red, ws.tiles);
-            if (threadIdx.x == 0) update_scalars(loc[q], HEAT, tot[0], tot[1], loc[q].kbase + kit);
+            group_sums<2>(bufB, ws.tile_begin, scene_lo, ns, comp, ws.tiles, red, [&](int q) { return (bool)loc[q].live; },
+                          [&](int q, const double(&tot)[2]) { update_scalars(loc[q], HEAT, tot[0], tot[1], loc[q].kbase + kit); });
         }
         if (threadIdx.x == 0) {
             int any = 0;
