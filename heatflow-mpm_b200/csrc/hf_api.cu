@@ -163,7 +163,7 @@ int encode_map(CUtensorMap* m, const float* base, int nk, int nj, int ni, int bk
 
 // The six TMA descriptors of a scene's tiled pressure stencil (order of hf::TileMaps): z and both search-direction
 // buffers with a one-cell halo, alpha_f x on its face lattice, alpha_f y and z in cell layout.
-static_assert(sizeof(hf::TileMaps) == 10 * sizeof(CUtensorMap), "TileMaps is ten consecutive descriptors");
+static_assert(sizeof(hf::TileMaps) == 12 * sizeof(CUtensorMap), "TileMaps is twelve consecutive descriptors");
 
 // a 3-D byte array (k fastest) of dims (nk, nj, ni) with a box (bk, bj, bi): nk and bk multiples of 16
 int encode_map_u8(CUtensorMap* m, const uint8_t* base, int nk, int nj, int ni, int bk, int bj, int bi) {
@@ -195,6 +195,8 @@ int encode_heat_maps(const hf_scene& sc, hf::TileMaps& m) {
     if ((rc = encode_map(&m.hkx, sc.hkx, n, n, n + 1, 32, 8, 5))) return rc;
     if ((rc = encode_map(&m.hky, sc.hky, n, n + 1, n, 32, 9, 4))) return rc;
     if ((rc = encode_map(&m.hkzc, sc.hkzc, n, n, n, 36, 8, 4))) return rc;
+    if ((rc = encode_map(&m.t0, sc.T[0], n, n, n, 40, 10, 6))) return rc;
+    if ((rc = encode_map(&m.t1, sc.T[1], n, n, n, 40, 10, 6))) return rc;
     return encode_map_u8(&m.flags, sc.cell_flags, n, n, n, 64, 10, 6);
 }
 

@@ -1483,6 +1483,43 @@ finish:
 // of the own cells is read from the staged box (its centre), A p is parked in the p_{k-1} box (dead once p_k is
 // formed), so a thread keeps only x, r and D of its cells in registers.  One group reduction per phase covers all the
 // thread's tiles.
+// Set-up of one heat cell from the staged boxes (x0 with a one-cell halo at B, then the face-diffusivity boxes and the
+// flag byte box at F): setup_cell<true>'s operations in its order on the same values (heat.py:198-203 with k_heat_diag
+// and neighbour_terms, use_fixed = 0).  Box offsets as in the iterations' stencil.
+__device__ __forceinline__ void heat_setup_box(const float* __restrict__ B, const float* __restrict__ F, float b, float c_dt,
+                                               const Cell& cl, int n, int bi, int bj, int bk, float& bo, float& d,
+                                               float& r, float& xo) {
+    const float* axb = F;
+    const float* ayb = axb + kBX;
+    const float* azb = ayb + kBY;
+    const unsigned char* flb = reinterpret_cast<const unsigned char*>(azb + kBW);
+    const int o = (bi + 1) * 400 + (bj + 1) * 40 + (bk + 4);
+    const int of = (bi + 1) * 640 + (bj + 1) * 64 + (bk + 16);
+    const float xc = B[o];
+    bo = b;
+    xo = xc;
+    if (flb[of] & 1) {
+        d = 1.0f;
+        r = __fsub_rn(b, xc);
+        return;
+    }
+    const bool in[6] = {cl.i > 0, cl.i < n - 1, cl.j > 0, cl.j < n - 1, cl.k > 0, cl.k < n - 1};
+    const float kf[6] = {axb[bi * 256 + bj * 32 + bk], axb[(bi + 1) * 256 + bj * 32 + bk], ayb[bi * 288 + bj * 32 + bk],
+                         ayb[bi * 288 + (bj + 1) * 32 + bk], azb[bi * 288 + bj * 36 + bk], azb[bi * 288 + bj * 36 + bk + 1]};
+    const int step[6] = {-400, 400, -40, 40, -1, 1}, fstep[6] = {-640, 640, -64, 64, -1, 1};
+    float sd = 0.0f, nt = 0.0f;
+#pragma unroll
+    for (int s = 0; s < 6; ++s)
+        if (in[s]) sd = __fadd_rn(sd, kf[s]);
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        if (!in[s]) continue;
+        nt = __fadd_rn(nt, (flb[of + fstep[s]] & 1) ? __fmul_rn(kf[s], xc) : __fmul_rn(kf[s], __fsub_rn(xc, B[o + step[s]])));
+    }
+    d = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(c_dt, sd)));
+    r = __fsub_rn(b, __fadd_rn(xc, __fmul_rn(c_dt, nt)));
+}
+
 template <bool HEAT, int MAXC>
 __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     k_pcg_tma(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, int tile_lo, int tile_hi,
@@ -1547,6 +1584,32 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
     }
     __syncthreads();
     float x[CPT], r[CPT], D[CPT];
+    // heat: x0 (the advected T, into the z slot), the face diffusivities and the cell flags with halo are staged by
+    // TMA before the set-up, which then reads them from shared memory; the coefficient boxes stay for the whole solve
+    if (HEAT) {
+        if (lt == 0) {
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < MAXC; ++q) {
+                if (!have[q]) continue;
+                float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
+                unsigned long long* mb = &mbar[g * MAXC + q];
+                mbar_expect_tx(mb, (unsigned)((kBZ + kBX + kBY + kBW) * sizeof(float) + kBF));
+                tma_load_3d(slot, (par ^ 1) ? &maps.t1 : &maps.t0, my[q].k0 - 4, my[q].j0 - 1, my[q].i0 - 1, mb);
+                tma_load_3d(slot + 2 * kBZ, &maps.hkx, my[q].k0, my[q].j0, my[q].i0, mb);
+                tma_load_3d(slot + 2 * kBZ + kBX, &maps.hky, my[q].k0, my[q].j0, my[q].i0, mb);
+                tma_load_3d(slot + 2 * kBZ + kBX + kBY, &maps.hkzc, my[q].k0, my[q].j0, my[q].i0, mb);
+                tma_load_3d(slot + 2 * kBZ + kBX + kBY + kBW, &maps.flags, my[q].k0 - 16, my[q].j0 - 1, my[q].i0 - 1, mb);
+            }
+        }
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < MAXC; ++q)
+            if (have[q]) ok = mbar_wait(&mbar[g * MAXC + q], phase_bit) && ok;
+        if (!ok) atomicExch(ws.err, 1);
+        phase_bit ^= 1u;
+    }
     // ------------------------------------------------------------------------------------------ prologue
     float mean = 0.0f;
     if (!HEAT) {
@@ -1566,10 +1629,16 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
                 x[s] = r[s] = D[s] = 0.0f;
                 const Cell cl = tile_cell(my[q], n, lt, m);
                 if (!have[q] || !cl.ok) continue;
-                float b, d, rr;
-                setup_cell<HEAT>(S, xg, mean, hh, c_dt, cl, b, d, rr);
+                float b, d, rr, xc;
+                if (HEAT) {
+                    const float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
+                    heat_setup_box(slot, slot + 2 * kBZ, S.hrhs[cl.t], c_dt, cl, n, m, lt >> 5, lt & 31, b, d, rr, xc);
+                } else {
+                    setup_cell<HEAT>(S, xg, mean, hh, c_dt, cl, b, d, rr);
+                    xc = xg[cl.t];
+                }
                 const float z = __fmul_rn(d, rr);
-                x[s] = xg[cl.t];
+                x[s] = xc;
                 D[s] = d;
                 r[s] = rr;
                 zg[cl.t] = z;
@@ -1589,23 +1658,20 @@ __global__ void __launch_bounds__(MAXC == 1 ? 1024 : (MAXC == 2 ? 768 : 512), 1)
             }
         }
     }
-    // the tiles' face coefficients stay in shared memory for the whole solve: face fractions (pressure), or the face
-    // diffusivities and the fixed-cell flags with a one-cell halo (heat)
-    if (lt == 0) {
+    // the tiles' face fractions stay in shared memory for the whole solve (heat: staged before the set-up)
+    if (!HEAT && lt == 0) {
 #pragma unroll
         for (int q = 0; q < MAXC; ++q) {
             if (!have[q]) continue;
             float* slot = sm_boxes + (size_t)(g * MAXC + q) * SLOT;
             unsigned long long* mb = &mbar[g * MAXC + q];
-            mbar_expect_tx(mb, (unsigned)((kBX + kBY + kBW) * sizeof(float) + (HEAT ? kBF : 0)));
-            tma_load_3d(slot + 2 * kBZ, HEAT ? &maps.hkx : &maps.ax, my[q].k0, my[q].j0, my[q].i0, mb);
-            tma_load_3d(slot + 2 * kBZ + kBX, HEAT ? &maps.hky : &maps.ayc, my[q].k0, my[q].j0, my[q].i0, mb);
-            tma_load_3d(slot + 2 * kBZ + kBX + kBY, HEAT ? &maps.hkzc : &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
-            if (HEAT)
-                tma_load_3d(slot + 2 * kBZ + kBX + kBY + kBW, &maps.flags, my[q].k0 - 16, my[q].j0 - 1, my[q].i0 - 1, mb);
+            mbar_expect_tx(mb, (unsigned)((kBX + kBY + kBW) * sizeof(float)));
+            tma_load_3d(slot + 2 * kBZ, &maps.ax, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + 2 * kBZ + kBX, &maps.ayc, my[q].k0, my[q].j0, my[q].i0, mb);
+            tma_load_3d(slot + 2 * kBZ + kBX + kBY, &maps.azc, my[q].k0, my[q].j0, my[q].i0, mb);
         }
     }
-    {
+    if (!HEAT) {
         bool ok = true;
 #pragma unroll
         for (int q = 0; q < MAXC; ++q)

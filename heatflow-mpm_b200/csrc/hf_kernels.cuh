@@ -40,6 +40,7 @@ struct Workspace {
 struct TileMaps {
     CUtensorMap z, p0, p1, ax, ayc, azc;      // pressure (and the z / p boxes of the heat system)
     CUtensorMap hkx, hky, hkzc, flags;        // heat: face diffusivities and the cell flags (bytes)
+    CUtensorMap t0, t1;                       // heat: both temperature buffers (x0 is the one the parity selects)
 };
 
 __global__ void k_scatter(const hf_scene* __restrict__ scenes, int s);
