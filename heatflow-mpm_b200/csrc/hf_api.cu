@@ -542,7 +542,7 @@ int hf_divergence_stage(const hf_plan* p, double dt, void* stream) {
     int rc = check_plan(p);
     if (rc) return rc;
     if (!p->num_chunks) return HF_OK;
-    hf::k_divergence<<<p->num_chunks, hf::kThreads, 0, S(stream)>>>(static_cast<const hf_scene*>(p->scenes_dev),
+    hf::k_divergence<<<p->num_chunks, hf::kChunk, 0, S(stream)>>>(static_cast<const hf_scene*>(p->scenes_dev),
                                                                    static_cast<const hf::WorkItem*>(p->work_dev), dt,
                                                                    workspace(p));
     HF_CUDA(cudaGetLastError(), "launch (divergence)");

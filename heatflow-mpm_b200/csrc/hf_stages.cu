@@ -1,9 +1,10 @@
 // hf_stages.cu -- the non-iterative stages of the air substep, batched over a scene table.
 //
-// Every chunked kernel runs one 256-thread block per 1024-cell work item (scene, first cell); each thread takes the
-// cells first + tid + 256*m, m = 0..3, so that warps read consecutive k (the contiguous axis) and every global access
-// is coalesced.  Face stages are organised by cell: a thread owns the three low faces u(i,j,k), v(i,j,k), w(i,j,k)
-// of its cell and, on the last layer, the high wall face.
+// The chunked kernels run one block per 1024-cell work item (scene, first cell): 256 threads taking the cells
+// first + tid + 256*m, m = 0..3 (the divergence: 1024 threads, one cell each), so that warps read consecutive k (the
+// contiguous axis) and every global access is coalesced.  The sampling stages run one 512-thread block per CG tile
+// with the lattices around the tile staged in shared memory.  Face stages are organised by cell: a thread owns the
+// three low faces u(i,j,k), v(i,j,k), w(i,j,k) of its cell and, on the last layer, the high wall face.
 #include <climits>
 
 #include "hf_device.cuh"
@@ -651,8 +652,12 @@ size_t advect_tile_smem() { return 4 * (size_t)kFBox * sizeof(float); }
 
 // grid.py:82-91 k_divergence_rhs with scale rho/dt into rhs, plus the fp64 partial sum of the chunk for the mean of
 // grid.py:238-241 (reduced over the scene by the pressure CG kernel, in a fixed tree).
-__global__ void __launch_bounds__(kThreads) k_divergence(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
-                                                        double dt_d, Workspace ws) {
+__global__ void __launch_bounds__(kChunk) k_divergence(const hf_scene* __restrict__ scenes, const WorkItem* __restrict__ work,
+                                                     double dt_d, Workspace ws) {
+    // one cell per thread (1024 per chunk, so all of a cell's loads are in flight at once); the chunk's sum is then
+    // formed in the tree of a 256-thread pass -- thread lt adds cells lt, lt + 256, lt + 512, lt + 768 in order, warp
+    // butterfly, 8 warps in order -- from the values parked in shared memory
+    __shared__ float rv[kChunk];
     __shared__ double red[kThreads / 32];
     const int c = blockIdx.x;
     const WorkItem wi = work[c];
@@ -661,10 +666,8 @@ __global__ void __launch_bounds__(kThreads) k_divergence(const hf_scene* __restr
     const int par = S.state->parity;
     const float *u = S.u[par ^ 1], *v = S.v[par ^ 1], *w = S.w[par ^ 1];
     const float h = (float)S.h, scale = (float)(S.rho / dt_d);
-    double part[1] = {0.0};
-    for (int m = 0; m < kCellsPerThread; ++m) {
-        const int t = wi.first + threadIdx.x + m * kThreads;
-        if (t >= N) break;
+    const int t = wi.first + threadIdx.x;
+    if (t < N) {
         int i, j, k;
         cell_ijk(t, n, i, j, k);
         const int u0 = uidx(n, i, j, k), u1i = uidx(n, i + 1, j, k);
@@ -685,10 +688,27 @@ __global__ void __launch_bounds__(kThreads) k_divergence(const hf_scene* __restr
         d = __fdiv_rn(d, h);
         const float r = __fmul_rn(-scale, d);
         S.rhs[t] = r;
-        part[0] += (double)r;
+        rv[threadIdx.x] = r;
     }
-    block_sum<1>(part, red);
-    if (threadIdx.x == 0) ws.mean_part[c] = part[0];
+    __syncthreads();
+    if (threadIdx.x < kThreads) {
+        double part = 0.0;
+#pragma unroll
+        for (int m = 0; m < kCellsPerThread; ++m) {
+            if (wi.first + threadIdx.x + m * kThreads >= N) break;
+            part += (double)rv[threadIdx.x + m * kThreads];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < kThreads / 32; ++q) s += red[q];
+        ws.mean_part[c] = s;
+    }
 }
 
 // ---------------------------------------------------------------------------------------------- diagnostics
