@@ -43,9 +43,37 @@ class FrozenBody:
         return self.pos_t, self.vel_t
 
     def set_state(self, positions, velocities):
-        """Replace the particle state (host arrays or tensors; pinned host tensors copy asynchronously)."""
-        self.pos_t.copy_(torch.as_tensor(positions), non_blocking=True)
-        self.vel_t.copy_(torch.as_tensor(velocities), non_blocking=True)
+        """Replace the particle state (host arrays or tensors).  Pinned host tensors are uploaded on a side stream into
+        the one of two device buffer pairs that no queued work still reads -- the one the substep before the previous
+        call copied from -- so the upload overlaps the substep in flight; work issued afterwards on the current stream
+        (the next substep) waits for it.  Other inputs are copied in stream order."""
+        p, v = torch.as_tensor(positions), torch.as_tensor(velocities)
+        if p.is_cuda or v.is_cuda or not (p.is_pinned() and v.is_pinned()):
+            self.pos_t.copy_(p, non_blocking=True)
+            self.vel_t.copy_(v, non_blocking=True)
+            return
+        dev = torch.device(self.dev)
+        if getattr(self, "_up", None) is None:
+            self._up = torch.cuda.Stream(dev)
+            self._bufs = [(self.pos_t, self.vel_t), (torch.empty_like(self.pos_t), torch.empty_like(self.vel_t))]
+            self._free = [None, None]   # event after which no queued work reads the pair
+            self._k = 0
+        compute = torch.cuda.current_stream(dev)
+        k = self._k ^ 1               # the pair not holding the current state
+        if self._free[k] is not None:
+            self._up.wait_event(self._free[k])
+        with torch.cuda.stream(self._up):
+            self._bufs[k][0].copy_(p, non_blocking=True)
+            self._bufs[k][1].copy_(v, non_blocking=True)
+            ready = torch.cuda.Event()
+            ready.record(self._up)
+        # the current pair is read by work already queued on this stream (the substep issued since the last call)
+        freed = torch.cuda.Event()
+        freed.record(compute)
+        self._free[self._k] = freed
+        compute.wait_event(ready)
+        self._k = k
+        self.pos_t, self.vel_t = self._bufs[k]
 
     def material_outputs(self):
         return self.yield_t, self.visc_t
