@@ -679,13 +679,14 @@ __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, 
 }
 
 // Tiles c = first, first + step, ... < end of scenes still iterating, through two shared-memory slots: the boxes of the
-// next tile are requested (issue, thread 0) before the current tile is worked on, so the copy overlaps the work.
+// next tile are requested (issue, thread 0) before the current tile is worked on, so the copy overlaps the work.  Bit s
+// of ph is the phase the next wait on slot s expects.
 // `work` must end with a __syncthreads after its last read of the slot (the slot is refilled next).  A wait that times
 // out sets the error flag and waits once more for the copy, so that no copy is left in flight.
 template <class Issue, class Work>
 __device__ __forceinline__ void pipelined_tiles(int first, int end, int step, const LocalScene* loc, int scene_lo,
                                                 const TileItem* __restrict__ tiles, float* slots,
-                                                unsigned long long* mbar, unsigned* ph, int* err, Issue issue, Work work) {
+                                                unsigned long long* mbar, unsigned& ph, int* err, Issue issue, Work work) {
     auto next_live = [&](int c) {
         while (c < end && !loc[tiles[c].scene - scene_lo].live) c += step;
         return c;
@@ -695,11 +696,12 @@ __device__ __forceinline__ void pipelined_tiles(int first, int end, int step, co
     while (cur < end) {
         const int nxt = next_live(cur + step);
         if (nxt < end && threadIdx.x == 0) issue(nxt, slots + (si ^ 1) * kSlotFloats, &mbar[si ^ 1]);
-        if (!mbar_wait(&mbar[si], ph[si])) {
+        const unsigned phase = (ph >> si) & 1u;
+        if (!mbar_wait(&mbar[si], phase)) {
             if (threadIdx.x == 0) atomicExch(err, 1);
-            mbar_wait(&mbar[si], ph[si]);
+            mbar_wait(&mbar[si], phase);
         }
-        ph[si] ^= 1u;
+        ph ^= 1u << si;
         work(cur, slots + si * kSlotFloats);
         cur = nxt;
         si ^= 1;
@@ -718,7 +720,7 @@ template <bool HEAT, bool TMA>
 __device__ bool solve_group(const hf_scene* __restrict__ scenes, const TileItem* __restrict__ tiles, const int4 grp,
                             int lb, int nlb, unsigned* bar, unsigned& epoch, double dt_d, const Workspace& ws,
                             double* red, LocalScene* loc, unsigned char* s_par, int* s_any, float* slots,
-                            unsigned long long* mbar, unsigned* ph) {
+                            unsigned long long* mbar, unsigned& ph) {
     const int scene_lo = grp.x, scene_hi = grp.y, tile_lo = grp.z, tile_hi = grp.w;
     const int ns = scene_hi - scene_lo;
     double* bufA = ws.partA;
@@ -1151,7 +1153,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(const hf_scene* __restrict__ s
     __shared__ __align__(8) unsigned long long mbar[2];
     extern __shared__ __align__(128) float sm_raw[];
     float* slots = TMA ? align128_shared(sm_raw) : nullptr;
-    unsigned ph[2] = {0u, 0u};
+    unsigned ph = 0u;   // bit s: the phase the next wait on slot s's mbarrier expects (a register, not an array)
     if (TMA && threadIdx.x == 0) {
         mbar_init(&mbar[0], 1);
         mbar_init(&mbar[1], 1);
