@@ -103,71 +103,6 @@ __device__ __forceinline__ float sample_at(const float* __restrict__ a, GridPos 
     return s;
 }
 
-__device__ __forceinline__ float sample(const float* __restrict__ a, float px, float py, float pz, float ox, float oy,
-                                        float oz, const DivBy& h, int nx, int ny, int nz) {
-    return sample_at(a, grid_pos(px, py, pz, h), ox, oy, oz, nx, ny, nz);
-}
-
-// One axis of a trilinear sample: the lower node index and the weights of the two nodes, for the lattice offset 0
-// (face lattice along this axis: nodes 0..n) or 0.5 (cell lattice: nodes 0..n-1).  fields.py:14-15, 29-35.
-struct Axis {
-    int i0, i1;
-    float w0, f;
-};
-
-__device__ __forceinline__ Axis axis_at(float q, float off, int nmax) {
-    const float g = __fsub_rn(q, off);
-    const int i = (int)floorf(g);
-    const float f = __fsub_rn(g, (float)i);
-    return Axis{clampi(i, 0, nmax), clampi(i + 1, 0, nmax), __fsub_rn(1.0f, f), f};
-}
-
-// sample_at's eight terms from precomputed axes (the same operations in the same order, so the same bits)
-__device__ __forceinline__ float sample_axes(const float* __restrict__ a, const Axis& X, const Axis& Y, const Axis& Z,
-                                             int sx, int sy) {
-    float s = 0.0f;
-    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.w0), Z.w0), __ldg(a + X.i0 * sx + Y.i0 * sy + Z.i0)));
-    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.w0), Z.f), __ldg(a + X.i0 * sx + Y.i0 * sy + Z.i1)));
-    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.f), Z.w0), __ldg(a + X.i0 * sx + Y.i1 * sy + Z.i0)));
-    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.w0, Y.f), Z.f), __ldg(a + X.i0 * sx + Y.i1 * sy + Z.i1)));
-    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.w0), Z.w0), __ldg(a + X.i1 * sx + Y.i0 * sy + Z.i0)));
-    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.w0), Z.f), __ldg(a + X.i1 * sx + Y.i0 * sy + Z.i1)));
-    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.f), Z.w0), __ldg(a + X.i1 * sx + Y.i1 * sy + Z.i0)));
-    s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(X.f, Y.f), Z.f), __ldg(a + X.i1 * sx + Y.i1 * sy + Z.i1)));
-    return s;
-}
-
-// fields.py:68-72 (the three lattices at one point: one division per coordinate).  Along each axis the face lattice
-// (offset 0, nodes 0..n) and the two cell lattices (offset 0.5, nodes 0..n-1) share their node indices and weights,
-// so each axis is resolved twice instead of three times.
-__device__ __forceinline__ void sample_velocity(const float* __restrict__ u, const float* __restrict__ v,
-                                                const float* __restrict__ w, float px, float py, float pz,
-                                                const DivBy& h, int n, float* o) {
-    const GridPos q = grid_pos(px, py, pz, h);
-    const Axis x0 = axis_at(q.x, 0.0f, n), x5 = axis_at(q.x, 0.5f, n - 1);
-    const Axis y0 = axis_at(q.y, 0.0f, n), y5 = axis_at(q.y, 0.5f, n - 1);
-    const Axis z0 = axis_at(q.z, 0.0f, n), z5 = axis_at(q.z, 0.5f, n - 1);
-    o[0] = sample_axes(u, x0, y5, z5, n * n, n);               // u: (n+1, n, n)
-    o[1] = sample_axes(v, x5, y0, z5, (n + 1) * n, n);         // v: (n, n+1, n)
-    o[2] = sample_axes(w, x5, y5, z0, n * (n + 1), n + 1);     // w: (n, n, n+1)
-}
-
-// fields.py:111-116: departure point x - dt u(x - dt/2 u(x))
-__device__ __forceinline__ void backtrace(const float* __restrict__ u, const float* __restrict__ v,
-                                          const float* __restrict__ w, const float* x, const DivBy& h, int n, float dt,
-                                          float* o) {
-    float vel[3];
-    sample_velocity(u, v, w, x[0], x[1], x[2], h, n, vel);
-    const float hdt = __fmul_rn(0.5f, dt);
-    float y0 = __fsub_rn(x[0], __fmul_rn(hdt, vel[0]));
-    float y1 = __fsub_rn(x[1], __fmul_rn(hdt, vel[1]));
-    float y2 = __fsub_rn(x[2], __fmul_rn(hdt, vel[2]));
-    sample_velocity(u, v, w, y0, y1, y2, h, n, vel);
-    o[0] = __fsub_rn(x[0], __fmul_rn(dt, vel[0]));
-    o[1] = __fsub_rn(x[1], __fmul_rn(dt, vel[1]));
-    o[2] = __fsub_rn(x[2], __fmul_rn(dt, vel[2]));
-}
-
 // heat.py:50-52 -- harmonic face diffusivity; symmetric bit for bit in (a, b) because 2*a is exact
 __device__ __forceinline__ float face_kappa(float a, float b) {
     return __fdiv_rn(__fmul_rn(__fmul_rn(2.0f, a), b), __fadd_rn(__fadd_rn(a, b), 1.0e-12f));
@@ -182,32 +117,6 @@ __device__ __forceinline__ void cell_ijk(int t, int n, int& i, int& j, int& k) {
 }
 
 __device__ __forceinline__ float fx_to_float(long long v) { return __double2float_rn(__ll2double_rn(v) * kFxInv); }
-
-// ------------------------------------------------------------------------------------ deterministic block reduce
-// Sum of `v` over the block in a fixed tree (warp xor-butterfly, then warps in index order).  Result valid in every
-// thread.  `red` must hold kThreads/32 doubles per component.
-template <int K>
-__device__ __forceinline__ void block_sum(double (&v)[K], double* red) {
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) {
-#pragma unroll
-        for (int c = 0; c < K; ++c) red[c * (kThreads / 32) + warp] = v[c];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-        double s = 0.0;
-#pragma unroll
-        for (int q = 0; q < kThreads / 32; ++q) s += red[c * (kThreads / 32) + q];
-        v[c] = s;
-    }
-}
 
 // ------------------------------------------------------------------------------------------- memory ordering
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {

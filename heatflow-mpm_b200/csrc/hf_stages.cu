@@ -370,7 +370,7 @@ __device__ __forceinline__ float relax_face(float q, float af, float kf, float m
 // node.  A trilinear sample whose eight nodes fall in the box then reads box[lower - origin] and its +1 neighbours,
 // which hold lattice[clamp(lower)] and lattice[clamp(lower + 1)] -- exactly the nodes fields.py:16-28 reads after
 // clamping -- with 32-bit shared addresses and no clamps; a sample outside the box (a back-trace longer than the halo)
-// reads the lattice itself.  Positions, weights and the order of every operation are those of sample_axes, so the
+// reads the lattice itself.  Positions, weights and the order of every operation are those of sample_at, so the
 // results are the same bits as sampling the lattice directly (fields.py's clamped nodes).
 constexpr int kFH = 2;
 constexpr int kFBX = kTI + 2 * kFH + 1, kFBY = kTJ + 2 * kFH + 1, kFBZ = kTK + 2 * kFH + 1;   // 9 x 13 x 37
@@ -396,7 +396,8 @@ __device__ __forceinline__ bool in_box(const BAxis& X, const BAxis& Y, const BAx
            (unsigned)Z.b <= (unsigned)(kFBZ - 2);
 }
 
-// sample_axes' eight terms in its order, from a box or (outside it) from the lattice with the clamped nodes
+// sample_at's eight terms in its order (fields.py:29-35: weight ((wx * wy) * wz) * a, dx, dy, dz), from a box or
+// (outside it) from the lattice with the clamped nodes
 __device__ __forceinline__ float box_sample(const float* __restrict__ B, const float* __restrict__ a, const BAxis& X,
                                             const BAxis& Y, const BAxis& Z, int nx, int ny, int nz) {
     float v[8];
