@@ -124,3 +124,55 @@ def test_package_functions_read_only_bound_names():
     files += [os.path.join(ROOT, "__graft_entry__.py")] + glob.glob(os.path.join(ROOT, "oracle", "*.py"))
     found = [f for p in sorted(files) for f in _check_file(p)]
     assert not found, found
+
+
+def test_clock_sampler_with_a_fake_nvml(monkeypatch):
+    """bench.ClockSampler reads the SM clock and the clock-event reasons through NVML on a thread during the timed
+    region: the samples taken between start() and stop() are summarised (median clock, max clock, the reason names of
+    every bit seen).  A fake pynvml stands in for the driver here; it reports sw_power_cap (bit 0x4) and hw_slowdown
+    (0x8).  With no NVML at all the sampler falls back to nvidia-smi and, when that is missing too, returns None."""
+    import time
+    import types
+    sys.path.insert(0, ROOT)
+    import bench
+    class FakeNvml:
+        NVML_CLOCK_SM = 1
+        reads = 0
+
+        @staticmethod
+        def nvmlInit():
+            pass
+
+        @staticmethod
+        def nvmlDeviceGetHandleByIndex(i):
+            return ("gpu", i)
+
+        @classmethod
+        def nvmlDeviceGetClockInfo(cls, handle, kind):
+            cls.reads += 1
+            return 1800
+
+        @staticmethod
+        def nvmlDeviceGetMaxClockInfo(handle, kind):
+            return 1965
+
+        @staticmethod
+        def nvmlDeviceGetCurrentClocksEventReasons(handle):
+            return 0x4 | 0x8
+
+    monkeypatch.setitem(sys.modules, "pynvml", FakeNvml)
+    cs = bench.ClockSampler(0)
+    cs.start()
+    time.sleep(0.05)
+    out = cs.stop()
+    assert out is not None and out["source"] == "nvml"
+    assert out["samples"] >= 1 and FakeNvml.reads >= out["samples"]
+    assert out["sm_mhz"] == 1800 and out["sm_max_mhz"] == 1965
+    assert out["reasons"] == ["hw_slowdown", "sw_power_cap"]
+
+    broken = types.SimpleNamespace(nvmlInit=lambda: (_ for _ in ()).throw(RuntimeError("no driver")))
+    monkeypatch.setitem(sys.modules, "pynvml", broken)
+    monkeypatch.setenv("PATH", "/nonexistent")
+    cs = bench.ClockSampler(0)
+    cs.start()
+    assert cs.stop() is None
