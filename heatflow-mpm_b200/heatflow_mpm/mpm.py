@@ -46,7 +46,8 @@ class FrozenBody:
         """Replace the particle state (host arrays or tensors).  Pinned host tensors are uploaded on a side stream into
         the one of two device buffer pairs that no queued work still reads -- the one the substep before the previous
         call copied from -- so the upload overlaps the substep in flight; work issued afterwards on the current stream
-        (the next substep) waits for it.  Other inputs are copied in stream order."""
+        (the next substep) waits for it.  As with any asynchronous copy, the pinned tensors must not be rewritten until
+        that work has run.  Other inputs are copied in stream order."""
         p, v = torch.as_tensor(positions), torch.as_tensor(velocities)
         if p.is_cuda or v.is_cuda or not (p.is_pinned() and v.is_pinned()):
             self.pos_t.copy_(p, non_blocking=True)
